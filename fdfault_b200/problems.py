@@ -1,0 +1,305 @@
+"""Writer for fdfault ``.in`` problem files and their binary side files.
+
+The solver reads the sectioned text format that the fdfault Python module
+writes (``python/fdfault/problem.py:1449-1512`` and the per-section writers it
+calls).  This module produces the same format from a small in-memory
+description, so problems can be built without the reference's Python package
+(which is not installed on GPU hosts).  Section layout and value order follow
+the readers in the reference solver:
+
+* ``[fdfault.problem]``   src/problem.cpp:24-50
+* ``[fdfault.domain]``    src/domain.cpp:35-76
+* ``[fdfault.fields]``    src/fields.cpp:24-47
+* ``[fdfault.blockIJK]``  src/block.cpp:52-86
+* ``[fdfault.operator]``  src/block.cpp:87-107
+* ``[fdfault.interfaceN]`` src/interface.cpp:28-54
+* ``[fdfault.friction]``  src/friction.cpp:76-129
+* ``[fdfault.slipweak]``  src/slipweak.cpp:42-96
+* ``[fdfault.stz]``       src/stz.cpp:51-113
+* ``[fdfault.outputlist]`` src/outputlist.cpp:28-72
+* ``[fdfault.frontlist]`` src/frontlist.cpp:20-40
+
+Floating-point values are written with ``repr`` so that the solver's decimal
+to binary conversion reproduces exactly the double held here.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import os
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+
+def _f(x: float) -> str:
+    return repr(float(x))
+
+
+@dataclasses.dataclass
+class Pert:
+    """One parametric perturbation line: shape, time ramp t0, x0, dx, y0, dy, values."""
+
+    kind: str
+    t0: float
+    x0: float
+    dx: float
+    y0: float
+    dy: float
+    values: Tuple[float, ...]
+
+    def line(self) -> str:
+        return " ".join([self.kind] + [_f(v) for v in (self.t0, self.x0, self.dx, self.y0, self.dy)]
+                        + [_f(v) for v in self.values])
+
+
+def load(kind, t0, x0, dx, y0, dy, sn, s2, s3) -> Pert:
+    return Pert(kind, t0, x0, dx, y0, dy, (sn, s2, s3))
+
+
+def swparam(kind, t0, x0, dx, y0, dy, dc, mus, mud, c0=0.0, trup=0.0, tc=0.0) -> Pert:
+    return Pert(kind, t0, x0, dx, y0, dy, (dc, mus, mud, c0, trup, tc))
+
+
+def stzparam(kind, t0, x0, dx, y0, dy, v0, f0, a, muy, c0, R, beta, chiw, v1) -> Pert:
+    return Pert(kind, t0, x0, dx, y0, dy, (v0, f0, a, muy, c0, R, beta, chiw, v1))
+
+
+@dataclasses.dataclass
+class Block:
+    rho: float
+    lam: float
+    g: float
+    xb: Sequence[float]
+    lb: Sequence[float]
+    bounds: Sequence[str]
+    surfaces: Sequence[str] = ()
+    plastic: Tuple[float, float, float, float] = (0.5735, 0.0, 0.2867, 0.2775)  # mu, c, beta, eta
+
+
+@dataclasses.dataclass
+class Interface:
+    direction: str
+    idx1: Tuple[int, int, int]
+    idx2: Tuple[int, int, int]
+    kind: str
+    loads: List[Pert] = dataclasses.field(default_factory=list)
+    loadfile: str = "none"
+    perts: List[Pert] = dataclasses.field(default_factory=list)
+    paramfile: str = "none"
+    chi0: float = 0.0
+    statefile: str = "none"
+
+
+@dataclasses.dataclass
+class Output:
+    name: str
+    field: str
+    tm: int
+    tp: int
+    ts: int
+    xm: Tuple[int, int, int]
+    xp: Tuple[int, int, int]
+    xs: Tuple[int, int, int]
+
+
+@dataclasses.dataclass
+class Problem:
+    name: str
+    ndim: int
+    nx_block: Tuple[List[int], List[int], List[int]]
+    mode: int = 2
+    datadir: str = "data/"
+    nt: int = 0
+    dt: float = 0.0
+    ttot: float = 0.0
+    cfl: float = 0.3
+    ninfo: int = 1000000
+    rkorder: int = 3
+    sbporder: int = 4
+    material: str = "elastic"
+    s0: Tuple[float, ...] = (0.0,) * 6
+    loadfile: str = "none"
+    matfile: str = "none"
+    plastic_tensor: bool = False
+    cdiss: float = 0.0
+    blocks: Dict[Tuple[int, int, int], Block] = dataclasses.field(default_factory=dict)
+    interfaces: List[Interface] = dataclasses.field(default_factory=list)
+    outputs: List[Output] = dataclasses.field(default_factory=list)
+    front: Optional[Tuple[str, float]] = None
+
+    @property
+    def nblocks(self) -> Tuple[int, int, int]:
+        return tuple(len(v) for v in self.nx_block)  # type: ignore
+
+    @property
+    def nx(self) -> Tuple[int, int, int]:
+        return tuple(sum(v) for v in self.nx_block)  # type: ignore
+
+    def block_start(self, coords) -> Tuple[int, int, int]:
+        return tuple(sum(self.nx_block[d][: coords[d]]) for d in range(3))  # type: ignore
+
+    def text(self) -> str:
+        L: List[str] = []
+        L += ["[fdfault.problem]", self.name, self.datadir, str(self.nt), _f(self.dt), _f(self.ttot),
+              _f(self.cfl), str(self.ninfo), str(self.rkorder), ""]
+        nb = self.nblocks
+        L += ["[fdfault.domain]", str(self.ndim), str(self.mode), " ".join(str(v) for v in self.nx),
+              " ".join(str(v) for v in nb)]
+        for d in range(3):
+            L.append(" ".join(str(v) for v in self.nx_block[d]))
+        L += [str(len(self.interfaces))]
+        L += [" ".join(i.kind for i in self.interfaces)] if self.interfaces else [""]
+        L += [str(self.sbporder), self.material, ""]
+        L += ["[fdfault.fields]", " ".join(_f(v) for v in self.s0), self.loadfile, self.matfile,
+              str(int(self.plastic_tensor)), ""]
+        for i in range(nb[0]):
+            for j in range(nb[1]):
+                for k in range(nb[2]):
+                    b = self.blocks[(i, j, k)]
+                    L.append("[fdfault.block%d%d%d]" % (i, j, k))
+                    mat = [b.rho, b.lam, b.g]
+                    if self.material == "plastic":
+                        mat += list(b.plastic)
+                    L.append(" ".join(_f(v) for v in mat))
+                    L.append(" ".join(_f(v) for v in b.xb[: self.ndim]))
+                    L.append(" ".join(_f(v) for v in b.lb[: self.ndim]))
+                    L += list(b.bounds)
+                    surfs = list(b.surfaces) if b.surfaces else ["none"] * (2 * self.ndim)
+                    L += surfs
+                    L.append("")
+        if self.cdiss > 0.0:
+            L += ["[fdfault.operator]", _f(self.cdiss), ""]
+        for n, itf in enumerate(self.interfaces):
+            L += ["[fdfault.interface%d]" % n, itf.direction, " ".join(str(v) for v in itf.idx1),
+                  " ".join(str(v) for v in itf.idx2), ""]
+            if itf.kind != "locked":
+                L += ["[fdfault.friction]", str(len(itf.loads))] + [p.line() for p in itf.loads]
+                L += [itf.loadfile, ""]
+            if itf.kind == "slipweak":
+                L += ["[fdfault.slipweak]", str(len(itf.perts))] + [p.line() for p in itf.perts]
+                L += [itf.paramfile, ""]
+            elif itf.kind == "stz":
+                L += ["[fdfault.stz]", _f(itf.chi0), itf.statefile, str(len(itf.perts))]
+                L += [p.line() for p in itf.perts] + [itf.paramfile, ""]
+        L.append("[fdfault.outputlist]")
+        for o in self.outputs:
+            L += [o.name, o.field, "%d %d %d" % (o.tm, o.tp, o.ts)]
+            for d in range(3):
+                L.append("%d %d %d" % (o.xm[d], o.xp[d], o.xs[d]))
+        L += ["", ""]
+        L.append("[fdfault.frontlist]")
+        if self.front is None:
+            L.append("0")
+        else:
+            L += ["1", self.front[0], _f(self.front[1])]
+        L.append("")
+        return "\n".join(L) + "\n"
+
+    def write(self, path: str) -> str:
+        with open(path, "w") as fh:
+            fh.write(self.text())
+        return path
+
+
+# ---------------------------------------------------------------------------
+# workload builders (seeded synthetic inputs with the shapes of the benchmark
+# configurations)
+
+RHO, CS, CP = 2.67, 3.464, 6.0
+LAM = RHO * (CP ** 2 - 2.0 * CS ** 2)
+G = RHO * CS ** 2
+
+
+def mode2_rupture(nx: int = 401, ny: int = 201, h: float = 0.1, nt: int = 1000, name: str = "mode2",
+                  datadir: str = "data/", rkorder: int = 3, sbporder: int = 4, cfl: float = 0.3,
+                  mus: float = 0.677, mud: float = 0.525, dc: float = 0.4, sn: float = -120.0,
+                  s2: float = 70.0, nuc: float = 81.6, nuc_half: float = 1.5,
+                  barriers: bool = False, outputs: Sequence[Output] = ()) -> Problem:
+    """2D plane-strain mode-II rupture on a flat horizontal fault.
+
+    Two blocks of nx by ny nodes (grid spacing h km) meet on the y-normal
+    fault; slip-weakening friction; uniform normal and shear load plus a
+    centred nucleation patch of half-width nuc_half km where the shear load
+    is raised to ``nuc``; absorbing outer boundaries.
+    """
+    lx, ly = (nx - 1) * h, (ny - 1) * h
+    p = Problem(name=name, ndim=2, mode=2, nx_block=([nx], [ny, ny], [1]), datadir=datadir, nt=nt,
+                cfl=cfl, rkorder=rkorder, sbporder=sbporder)
+    p.blocks[(0, 0, 0)] = Block(RHO, LAM, G, (0.0, 0.0), (lx, ly),
+                                ["absorbing", "absorbing", "absorbing", "none"])
+    p.blocks[(0, 1, 0)] = Block(RHO, LAM, G, (0.0, ly), (lx, ly),
+                                ["absorbing", "absorbing", "none", "absorbing"])
+    itf = Interface("y", (0, 0, 0), (0, 1, 0), "slipweak")
+    itf.loads = [load("constant", 0.0, 0.0, 0.0, 0.0, 0.0, sn, s2, 0.0),
+                 load("boxcar", 0.0, 0.5 * lx, nuc_half, 0.0, 0.0, 0.0, nuc - s2, 0.0)]
+    itf.perts = [swparam("constant", 0.0, 0.0, 0.0, 0.0, 0.0, dc, mus, mud)]
+    if barriers:
+        itf.perts += [swparam("boxcar", 0.0, 0.0625 * lx, 0.0625 * lx, 0.0, 0.0, 0.0, 10000.0, 0.0),
+                      swparam("boxcar", 0.0, 0.9375 * lx, 0.0625 * lx, 0.0, 0.0, 0.0, 10000.0, 0.0)]
+    p.interfaces.append(itf)
+    p.outputs = list(outputs)
+    return p
+
+
+def lognormal_field(n0: int, n1: int, h: float, mean: float, sd: float, corr: float,
+                    seed: int) -> np.ndarray:
+    """Seeded log-normal random field with a Gaussian correlation length.
+
+    White Gaussian noise is filtered in Fourier space by a Gaussian kernel of
+    correlation length ``corr`` (same units as the grid spacing ``h``), scaled
+    to unit variance, and mapped to a log-normal field with the requested
+    arithmetic mean and standard deviation.
+    """
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal((n0, n1))
+    k0 = np.fft.fftfreq(n0, d=h)
+    k1 = np.fft.fftfreq(n1, d=h)
+    kk = k0[:, None] ** 2 + k1[None, :] ** 2
+    filt = np.exp(-0.5 * (2.0 * np.pi) ** 2 * kk * (corr ** 2) / 2.0)
+    g = np.real(np.fft.ifft2(np.fft.fft2(w) * filt))
+    g = (g - g.mean()) / (g.std() + 1e-300)
+    s2 = np.log1p((sd / mean) ** 2)
+    mu_ln = np.log(mean) - 0.5 * s2
+    return np.exp(mu_ln + np.sqrt(s2) * g)
+
+
+def planar3d(nx: int = 401, ny: int = 201, nz: int = 201, h: float = 0.1, nt: int = 1500,
+             name: str = "planar3d", datadir: str = "data/", workdir: str = ".", seed: int = 1234,
+             rkorder: int = 3, sbporder: int = 4, cfl: float = 0.3, mus_mean: float = 0.677,
+             mus_sd: float = 0.03, corr: float = 2.0, region: Tuple[float, float] = (20.0, 15.0),
+             nuc_half: float = 1.0, mud: float = 0.525, dc: float = 0.4, sn: float = -120.0,
+             s2: float = 70.0, nuc: float = 81.6, outputs: Sequence[Output] = ()) -> Problem:
+    """3D vertical strike-slip fault: two blocks of nx*ny*nz nodes split in y.
+
+    Static friction per fault node comes from a seeded log-normal field
+    (written to a slip-weakening parameter file); outside a frictional region
+    of ``region`` km (along strike, along dip) static friction is 10000; a
+    square nucleation patch of half-width ``nuc_half`` km sits at the centre.
+    The free surface is the z+ face; the other outer faces absorb.
+    """
+    lx, ly, lz = (nx - 1) * h, (ny - 1) * h, (nz - 1) * h
+    p = Problem(name=name, ndim=3, mode=2, nx_block=([nx], [ny, ny], [nz]), datadir=datadir, nt=nt,
+                cfl=cfl, rkorder=rkorder, sbporder=sbporder)
+    p.blocks[(0, 0, 0)] = Block(RHO, LAM, G, (0.0, 0.0, 0.0), (lx, ly, lz),
+                                ["absorbing", "absorbing", "absorbing", "none", "absorbing", "free"])
+    p.blocks[(0, 1, 0)] = Block(RHO, LAM, G, (0.0, ly, 0.0), (lx, ly, lz),
+                                ["absorbing", "absorbing", "none", "absorbing", "absorbing", "free"])
+    itf = Interface("y", (0, 0, 0), (0, 1, 0), "slipweak")
+    xc, zc = 0.5 * lx, 0.5 * lz
+    itf.loads = [load("constant", 0.0, 0.0, 0.0, 0.0, 0.0, sn, s2, 0.0),
+                 load("boxcar", 0.0, xc, nuc_half, zc, nuc_half, 0.0, nuc - s2, 0.0)]
+    itf.perts = [swparam("constant", 0.0, 0.0, 0.0, 0.0, 0.0, dc, 0.0, mud)]
+    # per-node static friction: log-normal inside the frictional region, barrier outside
+    xs = np.arange(nx) * h
+    zs = np.arange(nz) * h
+    mus = lognormal_field(nx, nz, h, mus_mean, mus_sd, corr, seed)
+    inside = (np.abs(xs[:, None] - xc) <= 0.5 * region[0]) & (np.abs(zs[None, :] - zc) <= 0.5 * region[1])
+    mus = np.where(inside, mus, 10000.0)
+    zero = np.zeros((nx, nz))
+    pfile = os.path.join(workdir, name + ".swparam")
+    np.stack([zero, mus, zero, zero, zero, zero]).astype("<f8").tofile(pfile)
+    itf.paramfile = pfile
+    p.interfaces.append(itf)
+    p.outputs = list(outputs)
+    return p
