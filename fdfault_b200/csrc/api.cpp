@@ -1,0 +1,201 @@
+// C ABI (include/fdfault_b200.h) over the Solver class.  No C++ exception
+// crosses this boundary: every entry point converts failures into a negative
+// status and keeps the message for fdf_last_error().
+#include "../../include/fdfault_b200.h"
+
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+#include "solver.hpp"
+
+struct fdf_handle {
+    fdf::Solver* s = nullptr;
+    std::string err;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+template <typename F>
+int guarded(fdf_handle* h, F&& f) {
+    if (!h || !h->s) return FDF_ERR_ARG;
+    try {
+        f(*h->s);
+        return 0;
+    } catch (const std::exception& e) {
+        h->err = e.what();
+        if (h->err.find("solver status") != std::string::npos) return FDF_ERR_SOLVER;
+        if (h->err.find("cuda") != std::string::npos || h->err.find("CUDA") != std::string::npos) return FDF_ERR_CUDA;
+        return FDF_ERR_ARG;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdf_create(const char* infile, int precision, int device, fdf_handle** out) {
+    if (!infile || !out) return FDF_ERR_ARG;
+    *out = nullptr;
+    try {
+        fdf_handle* h = new fdf_handle;
+        try {
+            h->s = new fdf::Solver(infile, precision, device);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+        return 0;
+    } catch (const std::exception& e) {
+        g_create_error = e.what();
+        std::string m = g_create_error;
+        if (m.find("cuda") != std::string::npos) return FDF_ERR_CUDA;
+        return FDF_ERR_INPUT;
+    }
+}
+
+void fdf_destroy(fdf_handle* h) {
+    if (!h) return;
+    try {
+        delete h->s;
+    } catch (...) {
+    }
+    delete h;
+}
+
+int fdf_get_info(fdf_handle* h, int* ints, double* dbls) {
+    if (!ints || !dbls) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) {
+        const auto& P = s.spec();
+        const auto& L = s.layout();
+        ints[0] = P.ndim;
+        ints[1] = P.mode;
+        ints[2] = P.nx[0];
+        ints[3] = P.nx[1];
+        ints[4] = P.nx[2];
+        ints[5] = L.nfields;
+        ints[6] = L.nfieldsp;
+        ints[7] = (int)P.ifaces.size();
+        ints[8] = s.nstages();
+        ints[9] = s.nt();
+        ints[10] = P.sbporder;
+        ints[11] = P.nblocks[0];
+        ints[12] = P.nblocks[1];
+        ints[13] = P.nblocks[2];
+        ints[14] = P.plastic() ? 1 : 0;
+        ints[15] = P.rkorder;
+        dbls[0] = s.dt();
+        dbls[1] = s.ttot();
+        dbls[2] = s.cfl();
+    });
+}
+
+int fdf_do_rk_stage(fdf_handle* h, double dt, int stage, double t) {
+    return guarded(h, [&](fdf::Solver& s) { s.do_rk_stage(dt, stage, t); });
+}
+
+int fdf_step(fdf_handle* h, int nsteps) {
+    if (nsteps < 0) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { s.step(nsteps); });
+}
+
+int fdf_solve(fdf_handle* h) {
+    return guarded(h, [&](fdf::Solver& s) { s.solve(); });
+}
+
+int fdf_get_step(fdf_handle* h, int* step) {
+    if (!step) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { *step = s.step_index(); });
+}
+
+int fdf_set_step(fdf_handle* h, int step) {
+    if (step < 0) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { s.set_step_index(step); });
+}
+
+int fdf_get_field(fdf_handle* h, int comp, int absolute, double* out) {
+    if (!out) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { s.get_field(comp, absolute != 0, out); });
+}
+
+int fdf_set_field(fdf_handle* h, int comp, const double* in) {
+    if (!in) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { s.set_field(comp, in); });
+}
+
+int fdf_get_rate(fdf_handle* h, int comp, double* out) {
+    if (!out) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { s.get_rate(comp, out); });
+}
+
+int fdf_set_rate(fdf_handle* h, int comp, const double* in) {
+    if (!in) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { s.set_rate(comp, in); });
+}
+
+int fdf_get_geometry(fdf_handle* h, int which, int comp, double* out) {
+    if (!out) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { s.get_geometry(which, comp, out); });
+}
+
+int fdf_fault_count(fdf_handle* h, int iface, int which, long long* n) {
+    if (!n) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) {
+        long long c = s.fault_count(iface, which);
+        if (c < 0) throw std::runtime_error("interface index out of range");
+        *n = c;
+    });
+}
+
+int fdf_get_fault(fdf_handle* h, int iface, int which, double* out) {
+    if (!out) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { s.get_fault(iface, which, out); });
+}
+
+int fdf_set_fault(fdf_handle* h, int iface, int which, const double* in) {
+    if (!in) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { s.set_fault(iface, which, in); });
+}
+
+int fdf_synchronize(fdf_handle* h) {
+    return guarded(h, [&](fdf::Solver& s) {
+        s.synchronize();
+        if (int st = s.check_status()) throw std::runtime_error("solver status " + std::to_string(st));
+    });
+}
+
+int fdf_time_steps(fdf_handle* h, int nsteps, double* ms) {
+    if (!ms || nsteps < 0) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { *ms = (double)s.time_steps(nsteps); });
+}
+
+int fdf_profile(fdf_handle* h, int on) {
+    return guarded(h, [&](fdf::Solver& s) { s.set_profile(on != 0); });
+}
+
+int fdf_profile_read(fdf_handle* h, int kernel, double* total_ms, long long* launches) {
+    if (!total_ms || !launches) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { s.profile_read(kernel, total_ms, launches); });
+}
+
+int fdf_use_fast_kernel(fdf_handle* h, int on, int* active) {
+    return guarded(h, [&](fdf::Solver& s) {
+        s.use_fast_kernel(on != 0);
+        if (active) *active = s.fast_kernel_active() ? 1 : 0;
+    });
+}
+
+int fdf_bytes_per_node_stage(fdf_handle* h, long long* bytes) {
+    if (!bytes) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { *bytes = s.bytes_per_node_stage(); });
+}
+
+const char* fdf_last_error(fdf_handle* h) {
+    if (!h) return g_create_error.c_str();
+    return h->err.c_str();
+}
+
+}  // extern "C"

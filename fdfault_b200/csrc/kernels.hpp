@@ -1,0 +1,84 @@
+// Host-callable launchers for the device kernels of the fdfault B200 path.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fdf_types.hpp"
+
+namespace fdf {
+
+// block geometry for the set-up kernels
+struct GeoBlock {
+    int lo[3], n[3];
+    double dx[3];
+    const double* surf[6];   // bounding surfaces, [ndim][sn0][sn1]
+    int sn0[6], sn1[6];
+};
+
+void launch_transfinite(const Layout& L, const GeoBlock& g, double* X, cudaStream_t s);
+void launch_metrics(const Layout& L, const GeoBlock& g, int order, const double* X, double* M, double* J, int* status,
+                    cudaStream_t s);
+void launch_face_normals(const Layout& L, int d, int at, int lo0, int n0, int lo1, int n1, int flip, double h0dx,
+                         const double* M, double* nx[3], double* dl, double* dl2, int at2, double h0dx2,
+                         cudaStream_t s);
+void launch_max_speed(const Layout& L, const GeoBlock& g, double cs, const double* M, unsigned long long* out,
+                      cudaStream_t s);
+template <typename T>
+void launch_stress_roundtrip(const Layout& L, T* F, const double* S, const double s0[6], cudaStream_t s);
+void launch_to_float(const double* a, float* b, long long n, cudaStream_t s);
+
+// arguments of the volume (rate + outer SAT + RK update) kernel
+template <typename T>
+struct VolumeArgs {
+    Layout L;
+    int order;
+    double cdiss;
+    double s0[6];
+    const T* F;        // fields at the start of the stage
+    T* Fn;             // fields at the end of the stage
+    T* DF;             // RK rate register, updated in place
+    const T* M;        // metric, [ndim*ndim][cstride]
+    const T* J;        // Jacobian
+    T* FP;             // plastic-only fields, updated in place on the last stage
+    const double* S;   // heterogeneous initial stress or null
+    double* ABS;       // absolute-stress staging for output, or null
+    int plastic_tensor;
+};
+
+// exact-order kernel: one thread per node, reference operation order
+template <typename T>
+void launch_volume_exact(const VolumeArgs<T>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s);
+
+// optimised FP32 3D kernel (2.5D tiles marching along x, shared-memory halos)
+void launch_volume_fast3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s);
+bool fast3d_supported(const Layout& L, const BlockDev& b, int order);
+
+// interface kernels
+template <typename T>
+struct IfaceArgs {
+    Layout L;
+    double s0[6];
+    const T* F;
+    T* Fn;
+    T* DF;
+    T* FP;
+    const double* S;
+    double* ABS;
+    int plastic_tensor;
+    int* status;
+    const BlockDev* blocks;   // host copy indices resolved into b1/b2 below
+};
+
+template <typename T>
+void launch_interface(const IfaceArgs<T>& a, const IfaceDev& itf, const BlockDev& b1, const BlockDev& b2,
+                      const StageArgs& sa, int no_sat, cudaStream_t s);
+
+// output helpers
+template <typename T>
+void launch_fetch_component(const Layout& L, const T* F, int comp, int add_stress, const double s0[6],
+                            const double* S, double* out, cudaStream_t s);
+template <typename T>
+void launch_store_component(const Layout& L, T* F, int comp, const double* in, cudaStream_t s);
+void launch_front(const IfaceDev& itf, double t, double value, cudaStream_t s);
+
+}  // namespace fdf

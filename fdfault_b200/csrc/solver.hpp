@@ -1,0 +1,141 @@
+// Host orchestration of one fdfault problem on one GPU.
+//
+// Construction mirrors problem::problem + domain::domain (src/problem.cpp:16-84,
+// src/domain.cpp:19-153): read the .in file, build the grid and metrics on the
+// device, boundary and interface normals, friction parameters, the time step,
+// the initial interface solve, the initial absolute-stress round trip and the
+// initial front.  do_rk_stage() is the drop-in for domain::do_rk_stage
+// (src/domain.cpp:228-305) and step() for one pass of the loop body of
+// problem::solve (src/problem.cpp:151-168).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "fdf_types.hpp"
+#include "input.hpp"
+#include "kernels.hpp"
+
+namespace fdf {
+
+class OutputList;
+
+class Solver {
+  public:
+    Solver(const std::string& infile, int precision, int device);
+    ~Solver();
+    Solver(const Solver&) = delete;
+    Solver& operator=(const Solver&) = delete;
+
+    // one Runge-Kutta stage of one time step (domain::do_rk_stage)
+    void do_rk_stage(double dt, int stage, double t);
+    // nsteps full steps starting at the current step counter
+    void step(int nsteps);
+    // the whole problem::solve loop including output units and fronts
+    void solve();
+    // reset the step counter (tests that drive stages directly)
+    void set_step_index(int i) { step_index_ = i; }
+    int step_index() const { return step_index_; }
+
+    // host <-> device access in the reference's unpadded node order
+    void get_field(int comp, bool absolute, double* out);
+    void set_field(int comp, const double* in);
+    void get_rate(int comp, double* out);
+    void set_rate(int comp, const double* in);
+    void get_geometry(int which, int comp, double* out);
+    // volume component as the output list writes it at step tstep (absolute stress)
+    void fetch_output_component(int comp, int tstep, double* out);
+    void get_fault(int iface, int which, double* out);
+    void set_fault(int iface, int which, const double* in);
+    long long fault_count(int iface, int which) const;
+
+    void synchronize();
+    int check_status();            // reads and clears the device status word
+    float time_steps(int nsteps);  // device time of nsteps steps, ms (CUDA events on the solver stream)
+    void set_profile(bool on);
+    void profile_read(int kernel, double* total_ms, long long* launches);
+    void use_fast_kernel(bool on) { fast_ = on; }
+    bool fast_kernel_active() const;
+
+    const ProblemSpec& spec() const { return P_; }
+    const Layout& layout() const { return L_; }
+    int precision() const { return precision_; }
+    double dt() const { return dt_; }
+    int nt() const { return nt_; }
+    int nstages() const { return nstages_; }
+    double ttot() const { return ttot_; }
+    double cfl() const { return cfl_; }
+    cudaStream_t stream() const { return stream_; }
+    const std::vector<IfaceDev>& ifaces() const { return ifaces_; }
+    const std::vector<BlockDev>& blocks() const { return blocks_; }
+    long long bytes_per_node_stage() const;
+
+    // raw device pointers (for output units and tests)
+    void* field_ptr() const { return F_[cur_]; }
+    const double* x_ptr() const { return X_; }
+
+  private:
+    friend class OutputList;
+    template <typename T>
+    void stage_impl(double dt, int stage, double t, bool for_step);
+    template <typename T>
+    void init_fields();
+    void setup_geometry();
+    void setup_boundaries();
+    void setup_interfaces();
+    void set_time_step();
+    void set_block_coefficients();
+    void initial_interface_solve();
+    void launch_volume(int b, const StageArgs& sa);
+    void fetch_to(void* devbuf, size_t bytes, void* host);
+    double* scratch(size_t n);
+
+    ProblemSpec P_;
+    Layout L_{};
+    int precision_ = 0;   // 0 exact FP64, 1 FP32 fields
+    int device_ = 0;
+    cudaStream_t stream_ = nullptr;
+    double dt_ = 0, ttot_ = 0, cfl_ = 0;
+    int nt_ = 0, nstages_ = 0;
+    double A_[5] = {0}, B_[5] = {0}, C_[6] = {0};
+    int step_index_ = 0;
+    bool fast_ = true;
+
+    // device buffers
+    void* F_[2] = {nullptr, nullptr};
+    int cur_ = 0;
+    void* DF_ = nullptr;
+    void* FP_ = nullptr;
+    void* M_ = nullptr;
+    void* J_ = nullptr;
+    double* M64_ = nullptr;
+    double* J64_ = nullptr;
+    double* X_ = nullptr;
+    double* S_ = nullptr;
+    double* ABS_ = nullptr;
+    int* status_ = nullptr;
+    double* scratch_ = nullptr;
+    size_t scratch_n_ = 0;
+    std::vector<void*> owned_;   // face normals, fault arrays, parameter shapes
+
+    std::vector<BlockDev> blocks_;
+    std::vector<IfaceDev> ifaces_;
+    std::unique_ptr<OutputList> out_;
+
+    // profiling
+    bool profile_ = false;
+    std::vector<cudaEvent_t> ev_pool_;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending_;
+    double prof_ms_[4] = {0, 0, 0, 0};
+    long long prof_n_[4] = {0, 0, 0, 0};
+    void prof_flush();
+    cudaEvent_t ev_get();
+    void* dalloc(size_t bytes);
+};
+
+void cuda_check(cudaError_t e, const char* what);
+
+}  // namespace fdf

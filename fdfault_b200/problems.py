@@ -214,14 +214,15 @@ G = RHO * CS ** 2
 def mode2_rupture(nx: int = 401, ny: int = 201, h: float = 0.1, nt: int = 1000, name: str = "mode2",
                   datadir: str = "data/", rkorder: int = 3, sbporder: int = 4, cfl: float = 0.3,
                   mus: float = 0.677, mud: float = 0.525, dc: float = 0.4, sn: float = -120.0,
-                  s2: float = 70.0, nuc: float = 81.6, nuc_half: float = 1.5,
+                  s2: float = 70.0, nuc_dtau: float = 11.6, nuc_half: float = 1.5,
                   barriers: bool = False, outputs: Sequence[Output] = ()) -> Problem:
     """2D plane-strain mode-II rupture on a flat horizontal fault.
 
     Two blocks of nx by ny nodes (grid spacing h km) meet on the y-normal
     fault; slip-weakening friction; uniform normal and shear load plus a
     centred nucleation patch of half-width nuc_half km where the shear load
-    is raised to ``nuc``; absorbing outer boundaries.
+    is raised by ``nuc_dtau`` (70 + 11.6 = 81.6 MPa by default); absorbing
+    outer boundaries.
     """
     lx, ly = (nx - 1) * h, (ny - 1) * h
     p = Problem(name=name, ndim=2, mode=2, nx_block=([nx], [ny, ny], [1]), datadir=datadir, nt=nt,
@@ -232,7 +233,7 @@ def mode2_rupture(nx: int = 401, ny: int = 201, h: float = 0.1, nt: int = 1000, 
                                 ["absorbing", "absorbing", "none", "absorbing"])
     itf = Interface("y", (0, 0, 0), (0, 1, 0), "slipweak")
     itf.loads = [load("constant", 0.0, 0.0, 0.0, 0.0, 0.0, sn, s2, 0.0),
-                 load("boxcar", 0.0, 0.5 * lx, nuc_half, 0.0, 0.0, 0.0, nuc - s2, 0.0)]
+                 load("boxcar", 0.0, 0.5 * lx, nuc_half, 0.0, 0.0, 0.0, nuc_dtau, 0.0)]
     itf.perts = [swparam("constant", 0.0, 0.0, 0.0, 0.0, 0.0, dc, mus, mud)]
     if barriers:
         itf.perts += [swparam("boxcar", 0.0, 0.0625 * lx, 0.0625 * lx, 0.0, 0.0, 0.0, 10000.0, 0.0),
@@ -269,7 +270,7 @@ def planar3d(nx: int = 401, ny: int = 201, nz: int = 201, h: float = 0.1, nt: in
              rkorder: int = 3, sbporder: int = 4, cfl: float = 0.3, mus_mean: float = 0.677,
              mus_sd: float = 0.03, corr: float = 2.0, region: Tuple[float, float] = (20.0, 15.0),
              nuc_half: float = 1.0, mud: float = 0.525, dc: float = 0.4, sn: float = -120.0,
-             s2: float = 70.0, nuc: float = 81.6, outputs: Sequence[Output] = ()) -> Problem:
+             s2: float = 70.0, nuc_dtau: float = 11.6, outputs: Sequence[Output] = ()) -> Problem:
     """3D vertical strike-slip fault: two blocks of nx*ny*nz nodes split in y.
 
     Static friction per fault node comes from a seeded log-normal field
@@ -288,7 +289,7 @@ def planar3d(nx: int = 401, ny: int = 201, nz: int = 201, h: float = 0.1, nt: in
     itf = Interface("y", (0, 0, 0), (0, 1, 0), "slipweak")
     xc, zc = 0.5 * lx, 0.5 * lz
     itf.loads = [load("constant", 0.0, 0.0, 0.0, 0.0, 0.0, sn, s2, 0.0),
-                 load("boxcar", 0.0, xc, nuc_half, zc, nuc_half, 0.0, nuc - s2, 0.0)]
+                 load("boxcar", 0.0, xc, nuc_half, zc, nuc_half, 0.0, nuc_dtau, 0.0)]
     itf.perts = [swparam("constant", 0.0, 0.0, 0.0, 0.0, 0.0, dc, 0.0, mud)]
     # per-node static friction: log-normal inside the frictional region, barrier outside
     xs = np.arange(nx) * h

@@ -1,0 +1,215 @@
+"""ctypes binding of the C ABI (include/fdfault_b200.h) and a host-side mirror
+of the reference's problem / domain interface.
+
+``Problem(infile)`` stands for ``problem::problem`` (src/problem.cpp:16),
+``Problem.solve()`` for ``problem::solve`` (src/problem.cpp:136) and
+``Problem.do_rk_stage(dt, stage, t)`` for ``domain::do_rk_stage``
+(src/domain.cpp:228).  Errors raise ``FdfaultError`` with the library's
+message, the way the reference aborts with a message.
+
+The native library must be present: importing this module on a machine where
+``libfdfault_b200.so`` has not been built raises instead of falling back to
+any other implementation.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfdfault_b200.so")
+
+FP64, FP32 = 0, 1
+GEOM_X, GEOM_METRIC, GEOM_JAC = 0, 1, 2
+(U, DU, V, S, SN, UX, DUX, VX, SX, STATE, DSTATE, DSTATEDT, TFRONT) = range(13)
+
+
+class FdfaultError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FdfaultError("native library %s is missing; build it with fdfault_b200/build.py" % path)
+    L = ctypes.CDLL(path)
+    c_int, c_double, c_ll = ctypes.c_int, ctypes.c_double, ctypes.c_longlong
+    P = ctypes.POINTER
+    dp = P(c_double)
+    L.fdf_create.argtypes = [ctypes.c_char_p, c_int, c_int, P(ctypes.c_void_p)]
+    L.fdf_destroy.argtypes = [ctypes.c_void_p]
+    L.fdf_destroy.restype = None
+    L.fdf_get_info.argtypes = [ctypes.c_void_p, P(c_int), dp]
+    L.fdf_do_rk_stage.argtypes = [ctypes.c_void_p, c_double, c_int, c_double]
+    L.fdf_step.argtypes = [ctypes.c_void_p, c_int]
+    L.fdf_solve.argtypes = [ctypes.c_void_p]
+    L.fdf_get_step.argtypes = [ctypes.c_void_p, P(c_int)]
+    L.fdf_set_step.argtypes = [ctypes.c_void_p, c_int]
+    L.fdf_get_field.argtypes = [ctypes.c_void_p, c_int, c_int, dp]
+    L.fdf_set_field.argtypes = [ctypes.c_void_p, c_int, dp]
+    L.fdf_get_rate.argtypes = [ctypes.c_void_p, c_int, dp]
+    L.fdf_set_rate.argtypes = [ctypes.c_void_p, c_int, dp]
+    L.fdf_get_geometry.argtypes = [ctypes.c_void_p, c_int, c_int, dp]
+    L.fdf_fault_count.argtypes = [ctypes.c_void_p, c_int, c_int, P(c_ll)]
+    L.fdf_get_fault.argtypes = [ctypes.c_void_p, c_int, c_int, dp]
+    L.fdf_set_fault.argtypes = [ctypes.c_void_p, c_int, c_int, dp]
+    L.fdf_synchronize.argtypes = [ctypes.c_void_p]
+    L.fdf_time_steps.argtypes = [ctypes.c_void_p, c_int, dp]
+    L.fdf_profile.argtypes = [ctypes.c_void_p, c_int]
+    L.fdf_profile_read.argtypes = [ctypes.c_void_p, c_int, dp, P(c_ll)]
+    L.fdf_use_fast_kernel.argtypes = [ctypes.c_void_p, c_int, P(c_int)]
+    L.fdf_bytes_per_node_stage.argtypes = [ctypes.c_void_p, P(c_ll)]
+    L.fdf_last_error.argtypes = [ctypes.c_void_p]
+    L.fdf_last_error.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Problem:
+    """One fdfault problem held on a GPU."""
+
+    def __init__(self, infile: str, precision: int = FP64, device: int = 0):
+        self._L = load_library()
+        h = ctypes.c_void_p()
+        rc = self._L.fdf_create(infile.encode(), precision, device, ctypes.byref(h))
+        if rc:
+            raise FdfaultError(self._L.fdf_last_error(None).decode())
+        self._h = h
+        self.precision = precision
+        ints = (ctypes.c_int * 16)()
+        dbls = (ctypes.c_double * 3)()
+        self._check(self._L.fdf_get_info(self._h, ints, dbls))
+        v = list(ints)
+        self.ndim, self.mode = v[0], v[1]
+        self.nx: Tuple[int, int, int] = (v[2], v[3], v[4])
+        self.nfields, self.nfieldsp, self.nifaces, self.nstages, self.nt = v[5], v[6], v[7], v[8], v[9]
+        self.sbporder = v[10]
+        self.nblocks = (v[11], v[12], v[13])
+        self.is_plastic = bool(v[14])
+        self.rkorder = v[15]
+        self.dt, self.ttot, self.cfl = list(dbls)
+        self.nxyz = self.nx[0] * self.nx[1] * self.nx[2]
+
+    def _check(self, rc: int) -> None:
+        if rc:
+            raise FdfaultError(self._L.fdf_last_error(self._h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._L.fdf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # --- time stepping -------------------------------------------------
+    def do_rk_stage(self, dt: float, stage: int, t: float) -> None:
+        self._check(self._L.fdf_do_rk_stage(self._h, dt, stage, t))
+
+    def step(self, nsteps: int = 1) -> None:
+        self._check(self._L.fdf_step(self._h, nsteps))
+
+    def solve(self) -> None:
+        self._check(self._L.fdf_solve(self._h))
+
+    @property
+    def step_index(self) -> int:
+        v = ctypes.c_int()
+        self._check(self._L.fdf_get_step(self._h, ctypes.byref(v)))
+        return v.value
+
+    @step_index.setter
+    def step_index(self, i: int) -> None:
+        self._check(self._L.fdf_set_step(self._h, i))
+
+    def synchronize(self) -> None:
+        self._check(self._L.fdf_synchronize(self._h))
+
+    def time_steps(self, nsteps: int) -> float:
+        ms = ctypes.c_double()
+        self._check(self._L.fdf_time_steps(self._h, nsteps, ctypes.byref(ms)))
+        return ms.value
+
+    def profile(self, on: bool) -> None:
+        self._check(self._L.fdf_profile(self._h, int(on)))
+
+    def profile_read(self, kernel: int) -> Tuple[float, int]:
+        ms, n = ctypes.c_double(), ctypes.c_longlong()
+        self._check(self._L.fdf_profile_read(self._h, kernel, ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    def use_fast_kernel(self, on: bool) -> bool:
+        act = ctypes.c_int()
+        self._check(self._L.fdf_use_fast_kernel(self._h, int(on), ctypes.byref(act)))
+        return bool(act.value)
+
+    def bytes_per_node_stage(self) -> int:
+        b = ctypes.c_longlong()
+        self._check(self._L.fdf_bytes_per_node_stage(self._h, ctypes.byref(b)))
+        return b.value
+
+    # --- state access --------------------------------------------------
+    def field(self, comp: int, absolute: bool = False) -> np.ndarray:
+        out = np.empty(self.nxyz)
+        self._check(self._L.fdf_get_field(self._h, comp, int(absolute), _dptr(out)))
+        return out
+
+    def set_field(self, comp: int, values: np.ndarray) -> None:
+        a = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+        assert a.size == self.nxyz
+        self._check(self._L.fdf_set_field(self._h, comp, _dptr(a)))
+
+    def rate(self, comp: int) -> np.ndarray:
+        out = np.empty(self.nxyz)
+        self._check(self._L.fdf_get_rate(self._h, comp, _dptr(out)))
+        return out
+
+    def set_rate(self, comp: int, values: np.ndarray) -> None:
+        a = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+        assert a.size == self.nxyz
+        self._check(self._L.fdf_set_rate(self._h, comp, _dptr(a)))
+
+    def geometry(self, which: int, comp: int = 0) -> np.ndarray:
+        out = np.empty(self.nxyz)
+        self._check(self._L.fdf_get_geometry(self._h, which, comp, _dptr(out)))
+        return out
+
+    def fault_count(self, iface: int, which: int) -> int:
+        n = ctypes.c_longlong()
+        self._check(self._L.fdf_fault_count(self._h, iface, which, ctypes.byref(n)))
+        return n.value
+
+    def fault(self, iface: int, which: int) -> Optional[np.ndarray]:
+        n = self.fault_count(iface, which)
+        if n == 0:
+            return None
+        out = np.empty(n)
+        self._check(self._L.fdf_get_fault(self._h, iface, which, _dptr(out)))
+        return out
+
+    def set_fault(self, iface: int, which: int, values: np.ndarray) -> None:
+        a = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+        assert a.size == self.fault_count(iface, which)
+        self._check(self._L.fdf_set_fault(self._h, iface, which, _dptr(a)))

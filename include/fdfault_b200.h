@@ -1,0 +1,136 @@
+/*
+ * fdfault_b200 -- C ABI of the B200 time-stepping path for fdfault problems.
+ *
+ * The reference solver (edaub/fdfault) advances a problem with
+ *   problem::problem(const char* filename)        src/problem.cpp:16
+ *   problem::solve()                               src/problem.cpp:136
+ *   domain::do_rk_stage(dt, stage, t, rk)          src/domain.hpp:26, src/domain.cpp:228
+ * and keeps its state in fields::f/df (src/fields.hpp:58-59) and the friction
+ * arrays of interface/friction (src/interface.hpp:66-73, src/friction.hpp:23-26),
+ * which its output units read through friend access (src/outputunit.cpp:771-889).
+ * The entry points below replace those calls: the state lives in GPU memory,
+ * every stage runs as sm_100a kernels, and the host sees plain pointers and
+ * sizes.  Every function returns 0 on success or a negative error code (no
+ * C++ exception crosses the boundary); fdf_last_error() gives the message.
+ * A handle may be used from one host thread at a time.
+ */
+#ifndef FDFAULT_B200_H
+#define FDFAULT_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fdf_handle fdf_handle;
+
+/* precision of the field storage and stencil arithmetic */
+#define FDF_PRECISION_FP64 0 /* FP64, the reference's operation order (bit-identical results) */
+#define FDF_PRECISION_FP32 1 /* FP32 fields, metrics and stencil; FP64 friction, slip and time */
+
+/* error codes */
+#define FDF_ERR_ARG (-1)     /* invalid argument */
+#define FDF_ERR_INPUT (-2)   /* problem file or side file rejected */
+#define FDF_ERR_CUDA (-3)    /* CUDA runtime error */
+#define FDF_ERR_SOLVER (-4)  /* device status: Newton failure, STZ melting, non-finite values */
+
+/* geometry selectors for fdf_get_geometry */
+#define FDF_GEOM_X 0      /* node coordinates, comp 0..ndim-1 */
+#define FDF_GEOM_METRIC 1 /* d xi_l / d x_m, comp l*ndim+m */
+#define FDF_GEOM_JAC 2    /* Jacobian */
+
+/* fault array selectors for fdf_get_fault / fdf_set_fault (friction.hpp:23-26,
+ * interface.hpp:66-73, stz.cpp:160-162, front.hpp) */
+#define FDF_FAULT_U 0        /* slip magnitude */
+#define FDF_FAULT_DU 1       /* RK register of slip */
+#define FDF_FAULT_V 2        /* slip rate magnitude */
+#define FDF_FAULT_S 3        /* shear traction magnitude */
+#define FDF_FAULT_SN 4       /* normal traction */
+#define FDF_FAULT_UX 5       /* slip components, (ndim-1) planes */
+#define FDF_FAULT_DUX 6      /* RK register of slip components */
+#define FDF_FAULT_VX 7       /* slip-rate components */
+#define FDF_FAULT_SX 8       /* shear traction components */
+#define FDF_FAULT_STATE 9    /* STZ effective temperature */
+#define FDF_FAULT_DSTATE 10  /* RK register of the state */
+#define FDF_FAULT_DSTATEDT 11/* state rate */
+#define FDF_FAULT_TFRONT 12  /* rupture time (-1 before rupture) */
+
+/* Replaces problem::problem (src/problem.cpp:16-84) including
+ * domain::domain (src/domain.cpp:19-153): reads the .in file and its side
+ * files, builds grid, metrics, normals, friction parameters and the time
+ * step on device `device`. */
+int fdf_create(const char* infile, int precision, int device, fdf_handle** out);
+
+/* Releases all device memory of the problem. */
+void fdf_destroy(fdf_handle* h);
+
+/* ints[0..15]: ndim, mode, nx, ny, nz, nfields, nfieldsp, nifaces, nstages,
+ *              nt, sbporder, nblocks x, y, z, plastic, rkorder
+ * dbls[0..2]: dt, ttot, cfl  (problem::set_time_step, src/problem.cpp:94-134) */
+int fdf_get_info(fdf_handle* h, int* ints, double* dbls);
+
+/* Replaces domain::do_rk_stage (src/domain.cpp:228-305): one Runge-Kutta
+ * stage with time step dt at step time t. */
+int fdf_do_rk_stage(fdf_handle* h, double dt, int stage, double t);
+
+/* Runs nsteps steps of the problem::solve loop body (src/problem.cpp:151-168):
+ * all stages, the absolute-stress output round trip and the front update,
+ * without writing output files. */
+int fdf_step(fdf_handle* h, int nsteps);
+
+/* Replaces problem::solve (src/problem.cpp:136-192): runs the remaining
+ * steps, writes the output units and the rupture fronts. */
+int fdf_solve(fdf_handle* h);
+
+/* Index of the next step to run. */
+int fdf_get_step(fdf_handle* h, int* step);
+int fdf_set_step(fdf_handle* h, int step);
+
+/* Field component comp (reference numbering, src/outputunit.cpp:123-156 /
+ * 193-204) in the reference's node order (i, j, k; k fastest), n = nx*ny*nz
+ * values.  absolute=1 adds the initial stress to stress components, as the
+ * output units see them. */
+int fdf_get_field(fdf_handle* h, int comp, int absolute, double* out);
+int fdf_set_field(fdf_handle* h, int comp, const double* in);
+
+/* RK rate register df (src/fields.hpp:59) */
+int fdf_get_rate(fdf_handle* h, int comp, double* out);
+int fdf_set_rate(fdf_handle* h, int comp, const double* in);
+
+/* Coordinates, metric and Jacobian (src/fields.hpp:60-62). */
+int fdf_get_geometry(fdf_handle* h, int which, int comp, double* out);
+
+/* Number of values of a fault array of interface iface (0 if absent). */
+int fdf_fault_count(fdf_handle* h, int iface, int which, long long* n);
+int fdf_get_fault(fdf_handle* h, int iface, int which, double* out);
+int fdf_set_fault(fdf_handle* h, int iface, int which, const double* in);
+
+/* Waits for all queued device work; returns FDF_ERR_SOLVER if a kernel set
+ * a status bit (Newton failure, melting, non-finite values). */
+int fdf_synchronize(fdf_handle* h);
+
+/* Device time of nsteps steps (CUDA events on the solver's stream), ms. */
+int fdf_time_steps(fdf_handle* h, int nsteps, double* ms);
+
+/* Per-kernel timing: with profiling on, each volume-kernel launch (kernel 0)
+ * and each stage's interface kernels (kernel 1) are bracketed by CUDA events
+ * on the solver's stream; read returns total milliseconds and launches. */
+int fdf_profile(fdf_handle* h, int on);
+int fdf_profile_read(fdf_handle* h, int kernel, double* total_ms, long long* launches);
+
+/* Choose between the tiled FP32 volume kernel (default) and the
+ * one-thread-per-node kernel for FP32 problems; active=1 if the tiled kernel
+ * will run. */
+int fdf_use_fast_kernel(fdf_handle* h, int on, int* active);
+
+/* Algorithmic bytes moved per node per stage by the volume kernel. */
+int fdf_bytes_per_node_stage(fdf_handle* h, long long* bytes);
+
+/* Message of the last failed call on h (or of the last failed fdf_create when
+ * h is null). */
+const char* fdf_last_error(fdf_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
