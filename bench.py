@@ -1,0 +1,337 @@
+"""Benchmark: node-stage updates per second of the fdfault time-stepping path.
+
+Workload (default): the 3D planar strike-slip rupture -- two blocks of
+401x201x201 nodes (h = 0.1 km) split by a vertical y-normal fault, slip
+weakening with a seeded log-normal static-friction field (mean 0.677, sd 0.03,
+2 km correlation length), 20x15 km frictional region, 2x2 km nucleation patch,
+RK3 -- in FP32 fields with FP64 friction.  One "step" is one full RK3 time step
+(3 stages) over all 32,401,602 nodes.  Inputs are synthetic (seeded); no
+dataset is involved.
+
+Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+Under torchrun each rank runs its own replica of the problem on its own GPU
+(the single-grid path does not shard), so ``value`` is the sum over ranks of
+node-stage updates divided by the slowest rank's time (weak scaling).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "node-stage updates/s"
+WORKLOAD = dict(nx=401, ny=201, nz=201, h=0.1)
+CPU_SAMPLE = dict(nx=101, ny=51, nz=51, h=0.4)
+PROFILE_TRAFFIC = os.path.join(HERE, "profiles", "volume_fast3d_planar3d.md")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=0)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def build_problem(workdir, nt, **size):
+    from fdfault_b200 import problems as P
+
+    prob = P.planar3d(nt=nt, name="planar3d", datadir=workdir + "/", workdir=workdir, seed=1234,
+                      nx=size["nx"], ny=size["ny"], nz=size["nz"], h=size["h"])
+    return prob.write(os.path.join(workdir, "planar3d.in")), prob
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            v = json.load(fh)["hbm_gbs"]
+        return float(v), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per node-stage of the volume kernel from the committed ncu summary, or None."""
+    try:
+        with open(PROFILE_TRAFFIC) as fh:
+            for line in fh:
+                if line.startswith("traffic_bytes_per_node_stage:"):
+                    return float(line.split(":")[1].split()[0])
+    except Exception:
+        pass
+    return None
+
+
+def cpu_reference_sample(workdir, nsteps, nproc):
+    """Runs the reference solver (or, without its binary, the C oracle) on a
+    bounded sample of the workload: nproc concurrent single-process runs of a
+    101x51x51-per-block instance of the same problem, each timing only its
+    time-stepping loop.  Returns (node-stage/s aggregate, kind, cores, seconds)."""
+    import oracle
+
+    runs = []
+    for r in range(nproc):
+        d = os.path.join(workdir, "cpu%d" % r)
+        os.makedirs(d, exist_ok=True)
+        infile, prob = build_problem(d, nsteps, **CPU_SAMPLE)
+        runs.append((d, infile, prob))
+    nodes = CPU_SAMPLE["nx"] * (2 * CPU_SAMPLE["ny"]) * CPU_SAMPLE["nz"]
+    if os.path.exists(oracle.REF_BIN):
+        kind = "reference"
+        procs = []
+        for d, infile, _ in runs:
+            tf = os.path.join(d, "timing.txt")
+            env = dict(os.environ, FDF_REF_TIMING=tf)
+            procs.append((subprocess.Popen([oracle.REF_BIN, infile], cwd=d, env=env, stdout=subprocess.DEVNULL,
+                                           stderr=subprocess.DEVNULL), tf))
+        secs = []
+        for p, tf in procs:
+            p.wait()
+            with open(tf) as fh:
+                secs.append(float(fh.read().split()[-1]))
+    else:
+        kind = "port"
+        code = ("import sys,time; sys.path.insert(0,%r); import oracle; o=oracle.Oracle(sys.argv[1]); "
+                "t=time.perf_counter(); o.run(int(sys.argv[2])); print(time.perf_counter()-t)") % HERE
+        procs = [subprocess.Popen([sys.executable, "-c", code, infile, str(nsteps)], stdout=subprocess.PIPE,
+                                  text=True) for _, infile, _ in runs]
+        secs = [float(p.communicate()[0].split()[-1]) for p in procs]
+    total = nodes * 3 * nsteps * nproc
+    return total / max(secs), kind, nproc, max(secs)
+
+
+def cpu_workers():
+    """Host threads to use: all cores, bounded by memory (~0.5 GB per sample run)."""
+    n = os.cpu_count() or 1
+    try:
+        mem = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES")
+        n = min(n, max(1, int(mem // (512 << 20))))
+    except (ValueError, OSError):
+        pass
+    return max(1, min(n, 128))
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    nproc = cpu_workers()
+    tmp = tempfile.mkdtemp(prefix="fdf_refarm_")
+    rates, secs = [], []
+    kind = None
+    for i in range(args.warmup + args.steps):
+        rate, kind, cores, s = cpu_reference_sample(os.path.join(tmp, "s%d" % i), 1, nproc)
+        if i >= args.warmup:
+            rates.append(rate)
+            secs.append(s)
+    value = float(np.mean(rates))
+    nodes = CPU_SAMPLE["nx"] * (2 * CPU_SAMPLE["ny"]) * CPU_SAMPLE["nz"]
+    sample = ("%d concurrent single-process runs of the same problem at 101x51x51 nodes per block, 1 RK3 step "
+              "each, per timed step; time-stepping loop only" % nproc)
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "node-stage/s", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(secs)),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "planar3d 2x401x201x201 (sampled at 2x101x51x51)", "nodes_per_sample": nodes * nproc},
+           "cpu_baseline": {"value": value, "unit": "node-stage/s", "cores": nproc, "kind": kind, "sample": sample},
+           "e2e": {"value": value, "unit": "node-stage/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from fdfault_b200 import solver as fs
+
+    precision = fs.FP32 if args.precision == "fp32" else fs.FP64
+    tmp = tempfile.mkdtemp(prefix="fdf_bench_%d_" % rank)
+    nsteps_total = args.warmup + args.steps + max(args.e2e_steps, 0) + 10
+    infile, prob = build_problem(tmp, nsteps_total, **WORKLOAD)
+    t_setup = time.perf_counter()
+    p = fs.Problem(infile, precision=precision, device=local)
+    t_setup = time.perf_counter() - t_setup
+    fast = p.use_fast_kernel(True)
+    nodes = p.nxyz
+    nstages = p.nstages
+    nblocks = int(np.prod(p.nblocks))
+    p.step(args.warmup)
+    p.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    p.profile(True)
+    ms = p.time_steps(args.steps)
+    vol_ms, vol_n = p.profile_read(0)
+    if_ms, if_n = p.profile_read(1)
+    p.profile(False)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    p.synchronize()   # raises if any kernel reported a solver status
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    node_stages = nodes * nstages * args.steps * world
+    value = node_stages / (ms * 1e-3)
+
+    # end to end through the C-ABI with host buffers: upload the state from
+    # pinned host memory, then per step read back the on-fault output arrays
+    # that the reference's output units write every step (V, U, S, Sn, Vx, Sx)
+    ke = args.e2e_steps if args.e2e_steps > 0 else max(10, args.steps // 4)
+    fields = [torch.empty(nodes, dtype=torch.float64, pin_memory=True) for _ in range(p.nfields)]
+    for c in range(p.nfields):
+        fields[c].numpy()[:] = p.field(c)
+    outs = {w: torch.empty(p.fault_count(0, w), dtype=torch.float64, pin_memory=True)
+            for w in (fs.V, fs.U, fs.S, fs.SN, fs.VX, fs.SX)}
+    h2d = sum(f.numel() * 8 for f in fields)
+    d2h = sum(o.numel() * 8 for o in outs.values())
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for c in range(p.nfields):
+        p.set_field(c, fields[c].numpy())
+    for _ in range(ke):
+        p.step(1)
+        for w, o in outs.items():
+            o.numpy()[:] = p.fault(0, w)
+    p.synchronize()
+    te = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([te], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        te = float(t.item())
+    e2e = nodes * nstages * ke * world / te
+
+    bps = p.bytes_per_node_stage()
+    peak, peak_kind = measured_peak()
+    vol_avg_ms = vol_ms / max(vol_n, 1)
+    bytes_per_launch = bps * nodes / nblocks
+    achieved = bytes_per_launch / (vol_avg_ms * 1e-3) / 1e9
+    traffic_pn = profiled_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": peak_kind, "kernel": "volume_fast3d" if fast else "volume_exact",
+                "algorithmic_bytes_per_node_stage": bps,
+                "traffic": (traffic_pn * nodes / nblocks) if traffic_pn else None}
+    launches = args.steps * nstages * (nblocks + p.nifaces)
+    out = {"metric": METRIC, "value": value, "unit": "node-stage/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32" if precision == fs.FP32 else "f64", "data": "synthetic",
+           "config": {"workload": "planar3d: 2 blocks 401x201x201, slip weakening, log-normal mus, RK3",
+                      "nodes": nodes, "stages_per_step": nstages, "l2": "inputs larger than L2 (5.96 GB/stage)",
+                      "parallelism": "replicas" if world > 1 else "single", "setup_s": t_setup},
+           "clocks": clk,
+           "e2e": {"value": e2e, "unit": "node-stage/s", "h2d_bytes_per_step": h2d / ke, "d2h_bytes_per_step": d2h,
+                   "steps": ke, "note": "state uploaded once from pinned host memory (bytes amortised per step); "
+                                        "on-fault output arrays read back every step"},
+           "gpu_launches": launches,
+           "kernel_ms": {"volume_avg": vol_avg_ms, "volume_launches": vol_n,
+                         "interface_avg_per_stage": if_ms / max(if_n, 1)},
+           "roofline": roofline}
+    p.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, kind, cores, secs = cpu_reference_sample(tempfile.mkdtemp(prefix="fdf_cpu_"), 2, cpu_workers())
+        out["cpu_baseline"] = {"value": rate, "unit": "node-stage/s", "cores": cores, "kind": kind,
+                               "sample": "%d concurrent single-process runs of the workload at 101x51x51 nodes per "
+                                         "block, 2 RK3 steps each; time-stepping loop only (%.1f s)" % (cores, secs)}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
