@@ -32,6 +32,8 @@ sys.path.insert(0, HERE)
 
 METRIC = "node-stage updates/s"
 WORKLOAD = dict(nx=401, ny=201, nz=201, h=0.1)
+# reduced instance of the same problem for ncu captures (4.1M nodes, still far larger than L2)
+PROFILE_WORKLOAD = dict(nx=201, ny=101, nz=101, h=0.2)
 CPU_SAMPLE = dict(nx=101, ny=51, nz=51, h=0.4)
 PROFILE_TRAFFIC = os.path.join(HERE, "profiles", "volume_fast3d_planar3d.md")
 
@@ -45,6 +47,8 @@ def parse():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0)
+    ap.add_argument("--size", default="full", choices=["full", "profile"],
+                    help="profile: 2x201x101x101 instance for ncu captures")
     return ap.parse_args()
 
 
@@ -233,7 +237,7 @@ def main():
     precision = fs.FP32 if args.precision == "fp32" else fs.FP64
     tmp = tempfile.mkdtemp(prefix="fdf_bench_%d_" % rank)
     nsteps_total = args.warmup + args.steps + max(args.e2e_steps, 0) + 10
-    infile, prob = build_problem(tmp, nsteps_total, **WORKLOAD)
+    infile, prob = build_problem(tmp, nsteps_total, **(WORKLOAD if args.size == "full" else PROFILE_WORKLOAD))
     t_setup = time.perf_counter()
     p = fs.Problem(infile, precision=precision, device=local)
     t_setup = time.perf_counter() - t_setup

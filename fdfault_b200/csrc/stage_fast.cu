@@ -1,21 +1,449 @@
-// Tiled FP32 volume kernel for 3D blocks (placeholder dispatch: the tiled
-// kernel is not enabled for any layout yet, so FP32 problems run the
-// one-thread-per-node kernel).
+// Tiled FP32 volume kernel for 3D blocks.
+//
+// Same discrete operator as the reference's calc_df_3d (src/block.cpp:
+// 1541-2050) plus the outer SAT (src/boundary.cpp:265-503) and the RK update
+// (src/fields.cpp:293-309), reorganised for bandwidth:
+//  * each CTA owns a TJ x TK tile of (j, k) columns of one block and marches
+//    along x through a chunk of planes;
+//  * the x-derivative inputs of a column -- the x fluxes F_x,c = J (m_x . sigma_c)
+//    paired with the velocity v_c -- are formed once per plane when the plane
+//    enters the stencil window and kept in a per-thread shared-memory ring
+//    deep enough for the 9-tap boundary closure rows;
+//  * the y and z derivative inputs (F_y,c | v_c and F_z,c | v_c pairs) of the
+//    current plane go into shared tiles with a halo of order-1 nodes;
+//  * the centre values, rate register and halo node of the next plane are
+//    loaded at the end of the current plane's iteration (two resident CTAs
+//    per SM overlap one CTA's loads with the other's arithmetic);
+//  * interior stencils are unrolled with immediate coefficients in the
+//    antisymmetric form c1 (u+1 - u-1) + c2 (u+2 - u-2) + c3 (u+3 - u-3);
+//    boundary closure rows use the tabulated rows;
+//  * the rate is accumulated in registers, the outer SAT added on face
+//    nodes, and f and df are written once.
+// Momentum rates use sum_d (dt/rho/dx_d)/J * D_d(J m_d . sigma), which is
+// algebraically the reference's conservative form; stress rates use the
+// velocity-gradient form of the same non-conservative terms.  Arithmetic is
+// FP32 with FMA contraction; the FP64 exact-order kernel is stage_exact.cu.
 #include <cuda_runtime.h>
 
+
 #include "kernels.hpp"
+#include "sbp_coeffs.cuh"
+#include "stage_common.cuh"
 
 namespace fdf {
 
+namespace {
+
+constexpr int TJ = 8, TK = 32, NT = TJ * TK;
+
+template <int ORDER>
+struct FastCfg {
+    static constexpr int H = ORDER - 1;
+    static constexpr int NB = 2 * H;        // closure rows per side
+    static constexpr int NTB = 3 * H;       // taps of a closure row
+    static constexpr int R = NTB + 1;       // ring depth
+    static constexpr int HN = 2 * H * (TK + TJ);   // halo nodes per plane
+    static constexpr int VH = TJ + 2 * H, VW = TK + 2 * H;
+    static constexpr int RING = R * 3 * NT;   // float2 entries
+    static constexpr int TY = 3 * VH * TK;    // float2
+    static constexpr int TZ = 3 * TJ * VW;    // float2
+    static constexpr size_t SMEM = sizeof(float2) * (RING + TY + TZ);
+};
+
+// interior first-derivative weights in antisymmetric form (src/fd.cpp:53-83):
+// D u_p = sum_n c_n (u_{p+n} - u_{p-n})
+template <int ORDER>
+__device__ __forceinline__ constexpr float inner_c(int n) {
+    return ORDER == 4 ? (n == 1 ? 0.75f : (n == 2 ? -0.15f : 1.f / 60.f))
+                      : (ORDER == 3 ? (n == 1 ? 2.f / 3.f : -1.f / 12.f) : 0.5f);
+}
+
+// fluxes J*(m_d . sigma_c) for c = x, y, z; s = sxx, sxy, sxz, syy, syz, szz
+__device__ __forceinline__ void fluxes(float J, float m0, float m1, float m2, const float s[6], float F[3]) {
+    F[0] = J * (m0 * s[0] + m1 * s[1] + m2 * s[2]);
+    F[1] = J * (m0 * s[1] + m1 * s[3] + m2 * s[4]);
+    F[2] = J * (m0 * s[2] + m1 * s[4] + m2 * s[5]);
+}
+
+struct RingPlane {   // raw values of one column at one plane, for the x ring
+    float s[6], v[3], m[3], J;
+};
+struct HaloNode {
+    float s[6], v[3], m[3], J;
+};
+
+template <int ORDER, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_fast3d(VolumeArgs<float> a, BlockDev B, StageArgs sa, int chunk) {
+    using C = FastCfg<ORDER>;
+    constexpr int H = C::H, R = C::R, NB = C::NB, NTB = C::NTB, VH = C::VH, VW = C::VW;
+    extern __shared__ float2 smem2[];
+    float2* ring = smem2;              // [R][3][NT]   (F_x,c , v_c)
+    float2* ty = ring + C::RING;       // [3][VH][TK]  (F_y,c , v_c)
+    float2* tz = ty + C::TY;           // [3][TJ][VW]  (F_z,c , v_c)
+
+    const Layout& L = a.L;
+    const int cs = (int)L.cstride;
+    const int n0 = B.n[0], n1 = B.n[1], n2 = B.n[2];
+    const int tid = threadIdx.x;
+    const int tk = tid % TK, tj = tid / TK;
+    // The last tile in j and in k is shifted to end on the block face so it
+    // holds every right-closure row together with all of that row's taps;
+    // closure rows near a face are written by the face tile only, other rows
+    // by their natural tile (rows computed twice are written once).
+    const bool lastk = blockIdx.x == gridDim.x - 1, lastj = blockIdx.y == gridDim.y - 1;
+    const int k0 = lastk ? n2 - TK : blockIdx.x * TK;
+    const int j0 = lastj ? n1 - TJ : blockIdx.y * TJ;
+    const int k = k0 + tk, j = j0 + tj;
+    const bool ownk = (k >= n2 - NB) ? lastk : (k / TK == (int)blockIdx.x);
+    const bool ownj = (j >= n1 - NB) ? lastj : (j / TJ == (int)blockIdx.y);
+    const bool owner = ownk && ownj;
+    const int ib = blockIdx.z * chunk;
+    const int ie = min(n0, ib + chunk);
+    if (ib >= ie) return;
+
+    const int s0 = (int)L.s0;
+    const int colbase = B.lo[0] * s0 + (B.lo[1] + j) * (int)L.s1 + (B.lo[2] + k);
+    const float* __restrict__ F = a.F;
+    const float* __restrict__ M = a.M;
+    const float* __restrict__ Jg = a.J;
+    float* __restrict__ DFg = a.DF;
+    float* __restrict__ Fn = a.Fn;
+
+    // halo node handled by this thread (fixed for the whole march)
+    int hj = 0, hk = 0, hkind = -1;   // 0: j-halo (F_y), 1: k-halo (F_z)
+    if (tid < C::HN) {
+        if (tid < 2 * H * TK) {
+            const int r = tid / TK, c = tid % TK;
+            hj = (r < H) ? (r - H) : (TJ + r - H);
+            hk = c;
+            hkind = 0;
+        } else {
+            const int t2 = tid - 2 * H * TK;
+            const int r = t2 / (2 * H), c = t2 % (2 * H);
+            hj = r;
+            hk = (c < H) ? (c - H) : (TK + c - H);
+            hkind = 1;
+        }
+        const int gj = j0 + hj, gk = k0 + hk;
+        if (gj < 0 || gj >= n1 || gk < 0 || gk >= n2) hkind = -1;
+    }
+    const int hbase = B.lo[0] * s0 + (B.lo[1] + j0 + hj) * (int)L.s1 + (B.lo[2] + k0 + hk);
+    const int hrow = (hkind == 0) ? 3 : 6;   // metric row y or z
+
+    float crho[3], cg2l[3], cg[3], clam[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        crho[d] = (float)B.coef[d][0];
+        cg2l[d] = (float)B.coef[d][1];
+        cg[d] = (float)B.coef[d][2];
+        clam[d] = (float)B.coef[d][3];
+    }
+    const float Acoef = (float)sa.A, Bcoef = (float)sa.B;
+    const bool jint = (j >= NB) && (j < n1 - NB);
+    const bool kint = (k >= NB) && (k < n2 - NB);
+
+    auto mintap = [&](int i) { return i < NB ? 0 : (i >= n0 - NB ? n0 - NTB : i - H); };
+    auto maxtap = [&](int i) { return i < NB ? NTB - 1 : (i >= n0 - NB ? n0 - 1 : i + H); };
+
+    auto load_ring = [&](int q, RingPlane& r) {
+        const int id = colbase + q * s0;
+#pragma unroll
+        for (int c = 0; c < 6; c++) r.s[c] = __ldg(F + (3 + c) * cs + id);
+#pragma unroll
+        for (int c = 0; c < 3; c++) r.v[c] = __ldg(F + c * cs + id);
+#pragma unroll
+        for (int c = 0; c < 3; c++) r.m[c] = __ldg(M + c * cs + id);
+        r.J = __ldg(Jg + id);
+    };
+    auto store_ring = [&](int q, const RingPlane& r) {
+        float Fx[3];
+        fluxes(r.J, r.m[0], r.m[1], r.m[2], r.s, Fx);
+        float2* slot = ring + (q % R) * 3 * NT + tid;
+#pragma unroll
+        for (int c = 0; c < 3; c++) slot[c * NT] = make_float2(Fx[c], r.v[c]);
+    };
+    auto load_center = [&](int i, float f[9], float m[9], float& Jc, float df[9]) {
+        const int id = colbase + i * s0;
+#pragma unroll
+        for (int c = 0; c < 9; c++) f[c] = __ldg(F + c * cs + id);
+#pragma unroll
+        for (int c = 0; c < 9; c++) m[c] = __ldg(M + c * cs + id);
+        Jc = __ldg(Jg + id);
+#pragma unroll
+        for (int c = 0; c < 9; c++) df[c] = DFg[c * cs + id];
+    };
+    auto load_halo = [&](int i, HaloNode& h) {
+        if (hkind < 0) return;
+        const int id = hbase + i * s0;
+#pragma unroll
+        for (int c = 0; c < 6; c++) h.s[c] = __ldg(F + (3 + c) * cs + id);
+#pragma unroll
+        for (int c = 0; c < 3; c++) h.v[c] = __ldg(F + c * cs + id);
+#pragma unroll
+        for (int c = 0; c < 3; c++) h.m[c] = __ldg(M + (hrow + c) * cs + id);
+        h.J = __ldg(Jg + id);
+    };
+
+    // prologue: the x window of the first plane, and the first plane's loads
+    int loaded = mintap(ib);
+    {
+        const int need = maxtap(ib);
+        while (loaded <= need) {
+            RingPlane r;
+            load_ring(loaded, r);
+            store_ring(loaded, r);
+            loaded++;
+        }
+    }
+    float f[9], m[9], Jc, df[9];
+    load_center(ib, f, m, Jc, df);
+    HaloNode hn;
+    load_halo(ib, hn);
+
+    for (int i = ib; i < ie; i++) {
+        // ---- complete the x window for plane i
+        {
+            const int need = maxtap(i);
+            while (loaded <= need) {   // only near the block's x faces
+                RingPlane r;
+                load_ring(loaded, r);
+                store_ring(loaded, r);
+                loaded++;
+            }
+        }
+        // ---- shared tiles of plane i: centre and halo node
+        {
+            float Fy[3], Fz[3];
+            fluxes(Jc, m[3], m[4], m[5], f + 3, Fy);
+            fluxes(Jc, m[6], m[7], m[8], f + 3, Fz);
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                ty[(c * VH + tj + H) * TK + tk] = make_float2(Fy[c], f[c]);
+                tz[(c * TJ + tj) * VW + tk + H] = make_float2(Fz[c], f[c]);
+            }
+        }
+        if (hkind >= 0) {
+            float Fh[3];
+            fluxes(hn.J, hn.m[0], hn.m[1], hn.m[2], hn.s, Fh);
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                if (hkind == 0)
+                    ty[(c * VH + hj + H) * TK + hk] = make_float2(Fh[c], hn.v[c]);
+                else
+                    tz[(c * TJ + hj) * VW + hk + H] = make_float2(Fh[c], hn.v[c]);
+            }
+        }
+        const bool more = i + 1 < ie;
+        __syncthreads();
+
+        // ---- derivatives: DFl[d][c] of the fluxes, Dv[d][c] of the velocities
+        float DFl[3][3], Dv[3][3];
+        if (i >= NB && i < n0 - NB) {
+            const float2* c0 = ring + tid;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                float af = 0.f, av = 0.f;
+#pragma unroll
+                for (int n = 1; n <= H; n++) {
+                    const float2 p = c0[(((i + n) % R) * 3 + c) * NT];
+                    const float2 q = c0[(((i - n) % R) * 3 + c) * NT];
+                    af = fmaf(inner_c<ORDER>(n), p.x - q.x, af);
+                    av = fmaf(inner_c<ORDER>(n), p.y - q.y, av);
+                }
+                DFl[0][c] = af;
+                Dv[0][c] = av;
+            }
+        } else {
+            const bool left = i < NB;
+            const int row = left ? i + 1 : n0 - i;
+            const int base = left ? 0 : n0 - 1, step = left ? 1 : -1;
+            const float sg = left ? 1.f : -1.f;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                float af = 0.f, av = 0.f;
+                for (int n = 0; n < NTB; n++) {
+                    const float cf = sbp_coef<float>(ORDER, row, n);
+                    const float2 p = ring[(((base + n * step) % R) * 3 + c) * NT + tid];
+                    af = fmaf(cf, p.x, af);
+                    av = fmaf(cf, p.y, av);
+                }
+                DFl[0][c] = sg * af;
+                Dv[0][c] = sg * av;
+            }
+        }
+        // closure rows this tile does not write (another tile owns them) may
+        // have taps outside the tile: give them the interior form, whose taps
+        // always lie in the tile and its halo, and discard the result
+        const bool jskip = !jint && !ownj;
+        const bool kskip = !kint && !ownk;
+        if (jint || jskip) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                float af = 0.f, av = 0.f;
+#pragma unroll
+                for (int n = 1; n <= H; n++) {
+                    const float2 p = ty[(c * VH + tj + H + n) * TK + tk];
+                    const float2 q = ty[(c * VH + tj + H - n) * TK + tk];
+                    af = fmaf(inner_c<ORDER>(n), p.x - q.x, af);
+                    av = fmaf(inner_c<ORDER>(n), p.y - q.y, av);
+                }
+                DFl[1][c] = af;
+                Dv[1][c] = av;
+            }
+        } else {
+            const bool left = j < NB;
+            const int row = left ? j + 1 : n1 - j;
+            const int base = (left ? 0 : n1 - 1) - j0 + H, step = left ? 1 : -1;
+            const float sg = left ? 1.f : -1.f;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                float af = 0.f, av = 0.f;
+                for (int n = 0; n < NTB; n++) {
+                    const float cf = sbp_coef<float>(ORDER, row, n);
+                    const float2 p = ty[(c * VH + base + n * step) * TK + tk];
+                    af = fmaf(cf, p.x, af);
+                    av = fmaf(cf, p.y, av);
+                }
+                DFl[1][c] = sg * af;
+                Dv[1][c] = sg * av;
+            }
+        }
+        if (kint || kskip) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                float af = 0.f, av = 0.f;
+#pragma unroll
+                for (int n = 1; n <= H; n++) {
+                    const float2 p = tz[(c * TJ + tj) * VW + tk + H + n];
+                    const float2 q = tz[(c * TJ + tj) * VW + tk + H - n];
+                    af = fmaf(inner_c<ORDER>(n), p.x - q.x, af);
+                    av = fmaf(inner_c<ORDER>(n), p.y - q.y, av);
+                }
+                DFl[2][c] = af;
+                Dv[2][c] = av;
+            }
+        } else {
+            const bool left = k < NB;
+            const int row = left ? k + 1 : n2 - k;
+            const int base = (left ? 0 : n2 - 1) - k0 + H, step = left ? 1 : -1;
+            const float sg = left ? 1.f : -1.f;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                float af = 0.f, av = 0.f;
+                for (int n = 0; n < NTB; n++) {
+                    const float cf = sbp_coef<float>(ORDER, row, n);
+                    const float2 p = tz[(c * TJ + tj) * VW + base + n * step];
+                    af = fmaf(cf, p.x, af);
+                    av = fmaf(cf, p.y, av);
+                }
+                DFl[2][c] = sg * af;
+                Dv[2][c] = sg * av;
+            }
+        }
+        __syncthreads();   // shared tiles are rewritten for the next plane
+
+        // ---- rate: df = A df + L(f)
+#pragma unroll
+        for (int c = 0; c < 9; c++) df[c] *= Acoef;
+        const float iJ = 1.f / Jc;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const float w = crho[d] * iJ;
+            const float ma = m[3 * d], mb = m[3 * d + 1], mc = m[3 * d + 2];
+            df[0] = fmaf(w, DFl[d][0], df[0]);
+            df[1] = fmaf(w, DFl[d][1], df[1]);
+            df[2] = fmaf(w, DFl[d][2], df[2]);
+            const float dvx = Dv[d][0], dvy = Dv[d][1], dvz = Dv[d][2];
+            df[3] += cg2l[d] * ma * dvx + clam[d] * (mb * dvy + mc * dvz);
+            df[4] += cg[d] * (ma * dvy + mb * dvx);
+            df[5] += cg[d] * (ma * dvz + mc * dvx);
+            df[6] += cg2l[d] * mb * dvy + clam[d] * (ma * dvx + mc * dvz);
+            df[7] += cg[d] * (mb * dvz + mc * dvy);
+            df[8] += cg2l[d] * mc * dvz + clam[d] * (ma * dvx + mb * dvy);
+        }
+        // ---- outer-face SATs (faces of the block only)
+        bool defer = false;
+        const bool face = (i == 0) | (i == n0 - 1) | (j == 0) | (j == n1 - 1) | (k == 0) | (k == n2 - 1);
+        if (face) {
+            const int pos[3] = {i, j, k};
+#pragma unroll
+            for (int fc = 0; fc < 6; fc++) {
+                const int d = fc / 2;
+                const bool at = (fc % 2 == 0) ? (pos[d] == 0) : (pos[d] == B.n[d] - 1);
+                if (!at) continue;
+                if (B.defer[fc]) defer = true;
+                if (!B.bactive[fc]) continue;
+                const int fa = (d == 0) ? j : i;
+                const int fb = (d == 2) ? j : k;
+                boundary_sat<float, 3, 2>(B, fc, fa, fb, (float)sa.dt, f, df, false);
+            }
+        }
+        if (owner) {
+            const int id = colbase + i * s0;
+#pragma unroll
+            for (int c = 0; c < 9; c++) DFg[c * cs + id] = df[c];
+            if (!defer) {
+                float fn[9];
+#pragma unroll
+                for (int c = 0; c < 9; c++) fn[c] = fmaf(Bcoef, df[c], f[c]);
+                if (sa.last && sa.plastic)
+                    finish_node<float>(L, B, sa, a.s0, a.S, nullptr, a.FP, a.plastic_tensor, id, fn, false);
+#pragma unroll
+                for (int c = 0; c < 9; c++) Fn[c * cs + id] = fn[c];
+            }
+        }
+        if (more) {
+            load_center(i + 1, f, m, Jc, df);
+            load_halo(i + 1, hn);
+        }
+    }
+}
+
+template <int ORDER, int MINB>
+void launch_order(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s) {
+    using C = FastCfg<ORDER>;
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(k_fast3d<ORDER, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)C::SMEM);
+        configured = true;
+    }
+    const int tk = (b.n[2] + TK - 1) / TK, tj = (b.n[1] + TJ - 1) / TJ;
+    // split the x march into chunks so the grid fills the GPU a few times over
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int slots = MINB * nsm;
+    int chunks = (4 * slots + tk * tj - 1) / (tk * tj);
+    if (chunks < 1) chunks = 1;
+    int chunk = (b.n[0] + chunks - 1) / chunks;
+    if (chunk < 16) chunk = 16;
+    chunks = (b.n[0] + chunk - 1) / chunk;
+    dim3 grid(tk, tj, chunks);
+    k_fast3d<ORDER, MINB><<<grid, NT, C::SMEM, s>>>(a, b, sa, chunk);
+}
+
+}  // namespace
+
 bool fast3d_supported(const Layout& L, const BlockDev& b, int order) {
-    (void)L;
-    (void)b;
-    (void)order;
-    return false;
+    if (L.ndim != 3 || L.nfields != 9) return false;
+    if (order < 2 || order > 4) return false;
+    if (b.n[1] < TJ || b.n[2] < TK) return false;
+    if (b.n[0] < 4 * order - 3) return false;
+    if (L.cstride * 9 >= (1LL << 31)) return false;   // 32-bit element offsets
+    return true;
 }
 
 void launch_volume_fast3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s) {
-    launch_volume_exact<float>(a, b, sa, s);
+    if (a.cdiss > 0.) {
+        launch_volume_exact<float>(a, b, sa, s);   // artificial dissipation: exact-order kernel
+        return;
+    }
+    switch (a.order) {
+        case 2: launch_order<2, 2>(a, b, sa, s); break;
+        case 3: launch_order<3, 2>(a, b, sa, s); break;
+        default: launch_order<4, 2>(a, b, sa, s); break;
+    }
 }
 
 }  // namespace fdf
