@@ -155,10 +155,10 @@ __global__ void __launch_bounds__(NT, MINB) k_fast3d(VolumeArgs<float> a, BlockD
         for (int c = 0; c < 3; c++) r.m[c] = __ldg(M + c * cs + id);
         r.J = __ldg(Jg + id);
     };
-    auto store_ring = [&](int q, const RingPlane& r) {
+    auto store_ring = [&](int qslot, const RingPlane& r) {
         float Fx[3];
         fluxes(r.J, r.m[0], r.m[1], r.m[2], r.s, Fx);
-        float2* slot = ring + (q % R) * 3 * NT + tid;
+        float2* slot = ring + qslot * 3 * NT + tid;
 #pragma unroll
         for (int c = 0; c < 3; c++) slot[c * NT] = make_float2(Fx[c], r.v[c]);
     };
@@ -186,15 +186,19 @@ __global__ void __launch_bounds__(NT, MINB) k_fast3d(VolumeArgs<float> a, BlockD
 
     // prologue: the x window of the first plane, and the first plane's loads
     int loaded = mintap(ib);
+    int lslot = loaded % R;
     {
         const int need = maxtap(ib);
         while (loaded <= need) {
             RingPlane r;
             load_ring(loaded, r);
-            store_ring(loaded, r);
+            store_ring(lslot, r);
             loaded++;
+            lslot = (lslot + 1 == R) ? 0 : lslot + 1;
         }
     }
+    int islot = ib % R;
+    const int rslot = (n0 - 1) % R;
     float f[9], m[9], Jc, df[9];
     load_center(ib, f, m, Jc, df);
     HaloNode hn;
@@ -207,8 +211,9 @@ __global__ void __launch_bounds__(NT, MINB) k_fast3d(VolumeArgs<float> a, BlockD
             while (loaded <= need) {   // only near the block's x faces
                 RingPlane r;
                 load_ring(loaded, r);
-                store_ring(loaded, r);
+                store_ring(lslot, r);
                 loaded++;
+                lslot = (lslot + 1 == R) ? 0 : lslot + 1;
             }
         }
         // ---- shared tiles of plane i: centre and halo node
@@ -245,8 +250,10 @@ __global__ void __launch_bounds__(NT, MINB) k_fast3d(VolumeArgs<float> a, BlockD
                 float af = 0.f, av = 0.f;
 #pragma unroll
                 for (int n = 1; n <= H; n++) {
-                    const float2 p = c0[(((i + n) % R) * 3 + c) * NT];
-                    const float2 q = c0[(((i - n) % R) * 3 + c) * NT];
+                    const int sp = (islot + n >= R) ? islot + n - R : islot + n;
+                    const int sq = (islot - n < 0) ? islot - n + R : islot - n;
+                    const float2 p = c0[(sp * 3 + c) * NT];
+                    const float2 q = c0[(sq * 3 + c) * NT];
                     af = fmaf(inner_c<ORDER>(n), p.x - q.x, af);
                     av = fmaf(inner_c<ORDER>(n), p.y - q.y, av);
                 }
@@ -263,7 +270,9 @@ __global__ void __launch_bounds__(NT, MINB) k_fast3d(VolumeArgs<float> a, BlockD
                 float af = 0.f, av = 0.f;
                 for (int n = 0; n < NTB; n++) {
                     const float cf = sbp_coef<float>(ORDER, row, n);
-                    const float2 p = ring[(((base + n * step) % R) * 3 + c) * NT + tid];
+                    int sl = left ? n : rslot - n;
+                    if (sl < 0) sl += R;
+                    const float2 p = ring[(sl * 3 + c) * NT + tid];
                     af = fmaf(cf, p.x, af);
                     av = fmaf(cf, p.y, av);
                 }
@@ -345,7 +354,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fast3d(VolumeArgs<float> a, BlockD
         // ---- rate: df = A df + L(f)
 #pragma unroll
         for (int c = 0; c < 9; c++) df[c] *= Acoef;
-        const float iJ = 1.f / Jc;
+        const float iJ = __frcp_rn(Jc);
 #pragma unroll
         for (int d = 0; d < 3; d++) {
             const float w = crho[d] * iJ;
@@ -396,6 +405,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fast3d(VolumeArgs<float> a, BlockD
             load_center(i + 1, f, m, Jc, df);
             load_halo(i + 1, hn);
         }
+        islot = (islot + 1 == R) ? 0 : islot + 1;
     }
 }
 
