@@ -121,6 +121,11 @@ int fdf_get_field(fdf_handle* h, int comp, int absolute, double* out) {
     return guarded(h, [&](fdf::Solver& s) { s.get_field(comp, absolute != 0, out); });
 }
 
+int fdf_get_field_noalloc(fdf_handle* h, int comp, int absolute, double* out) {
+    if (!out) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { s.get_field_noalloc(comp, absolute != 0, out); });
+}
+
 int fdf_set_field(fdf_handle* h, int comp, const double* in) {
     if (!in) return FDF_ERR_ARG;
     return guarded(h, [&](fdf::Solver& s) { s.set_field(comp, in); });

@@ -13,6 +13,7 @@
 #include <stdexcept>
 #include <unordered_map>
 
+#include "noalloc.hpp"
 #include "output.hpp"
 
 namespace fdf {
@@ -938,6 +939,23 @@ void Solver::get_field(int comp, bool absolute, double* out) {
     else
         launch_fetch_component<float>(L_, (const float*)base, c, absolute && comp < L_.nfields, P_.s0, S_, tmp, stream_);
     fetch_to(tmp, n * sizeof(double), out);
+}
+
+void Solver::get_field_noalloc(int comp, bool absolute, double* out) {
+    if (comp < 0 || comp >= L_.nfields + L_.nfieldsp) throw std::runtime_error("field component out of range");
+    const long long n = (long long)P_.nx[0] * P_.nx[1] * P_.nx[2];
+    if (n > FDF_NOALLOC_MAX_VALUES)
+        throw std::invalid_argument("field of " + std::to_string(n) + " values exceeds the allocation-free buffer (" +
+                                    std::to_string(FDF_NOALLOC_MAX_VALUES) + " values)");
+    double* buf = noalloc_field_buffer(device_);
+    // the gather kernel writes all n values: nothing has to start at zero
+    void* base = (comp < L_.nfields) ? F_[cur_] : FP_;
+    int c = (comp < L_.nfields) ? comp : comp - L_.nfields;
+    if (precision_ == 0)
+        launch_fetch_component<double>(L_, (const double*)base, c, absolute && comp < L_.nfields, P_.s0, S_, buf, stream_);
+    else
+        launch_fetch_component<float>(L_, (const float*)base, c, absolute && comp < L_.nfields, P_.s0, S_, buf, stream_);
+    fetch_to(buf, (size_t)n * sizeof(double), out);
 }
 
 void Solver::set_field(int comp, const double* in) {

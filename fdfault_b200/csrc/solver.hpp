@@ -42,6 +42,9 @@ class Solver {
 
     // host <-> device access in the reference's unpadded node order
     void get_field(int comp, bool absolute, double* out);
+    // same values as get_field, gathered into the fixed static device buffer
+    // (noalloc.hpp) instead of the growable scratch buffer; never allocates
+    void get_field_noalloc(int comp, bool absolute, double* out);
     void set_field(int comp, const double* in);
     void get_rate(int comp, double* out);
     void set_rate(int comp, const double* in);

@@ -55,6 +55,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fdf_get_step.argtypes = [ctypes.c_void_p, P(c_int)]
     L.fdf_set_step.argtypes = [ctypes.c_void_p, c_int]
     L.fdf_get_field.argtypes = [ctypes.c_void_p, c_int, c_int, dp]
+    L.fdf_get_field_noalloc.argtypes = [ctypes.c_void_p, c_int, c_int, dp]
     L.fdf_set_field.argtypes = [ctypes.c_void_p, c_int, dp]
     L.fdf_get_rate.argtypes = [ctypes.c_void_p, c_int, dp]
     L.fdf_set_rate.argtypes = [ctypes.c_void_p, c_int, dp]
@@ -174,6 +175,12 @@ class Problem:
     def field(self, comp: int, absolute: bool = False) -> np.ndarray:
         out = np.empty(self.nxyz)
         self._check(self._L.fdf_get_field(self._h, comp, int(absolute), _dptr(out)))
+        return out
+
+    def field_noalloc(self, comp: int, absolute: bool = False) -> np.ndarray:
+        """As field(), through the allocation-free entry point (fixed device buffer)."""
+        out = np.empty(self.nxyz)
+        self._check(self._L.fdf_get_field_noalloc(self._h, comp, int(absolute), _dptr(out)))
         return out
 
     def set_field(self, comp: int, values: np.ndarray) -> None:

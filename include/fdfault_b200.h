@@ -90,6 +90,17 @@ int fdf_set_step(fdf_handle* h, int step);
  * values.  absolute=1 adds the initial stress to stress components, as the
  * output units see them. */
 int fdf_get_field(fdf_handle* h, int comp, int absolute, double* out);
+
+/* Same values as fdf_get_field, without any device allocation: the component
+ * is gathered into one fixed static device buffer of FDF_NOALLOC_MAX_VALUES
+ * doubles (8 MiB) per device, then copied to `out`.  No counterpart in the
+ * reference (which has no device memory).  Fields larger than the buffer are
+ * rejected with FDF_ERR_ARG.  The buffer is shared by every handle on the
+ * device: calls that overlap in time (from several host threads, or on
+ * several handles of one device) race on it and may return each other's
+ * values; serialise them. */
+#define FDF_NOALLOC_MAX_VALUES 1048576
+int fdf_get_field_noalloc(fdf_handle* h, int comp, int absolute, double* out);
 int fdf_set_field(fdf_handle* h, int comp, const double* in);
 
 /* RK rate register df (src/fields.hpp:59) */
