@@ -198,6 +198,70 @@ int fdf_bytes_per_node_stage(fdf_handle* h, long long* bytes) {
     return guarded(h, [&](fdf::Solver& s) { *bytes = s.bytes_per_node_stage(); });
 }
 
+int fdf_stz_set_learned(fdf_handle* h, int on) {
+    return guarded(h, [&](fdf::Solver& s) { s.set_stz_learned(on != 0); });
+}
+
+int fdf_stz_set_counting(fdf_handle* h, int on) {
+    return guarded(h, [&](fdf::Solver& s) { s.set_stz_counting(on != 0); });
+}
+
+int fdf_stz_read_counts(fdf_handle* h, long long* counts, int reset) {
+    if (!counts) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { s.read_stz_counts(counts, reset != 0); });
+}
+
+int fdf_stz_collect(fdf_handle* h, long long capacity) {
+    return guarded(h, [&](fdf::Solver& s) { s.stz_collect(capacity); });
+}
+
+int fdf_stz_samples(fdf_handle* h, float* out, long long max_rows, long long* count) {
+    if (!count || max_rows < 0 || (max_rows > 0 && !out)) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { *count = s.stz_samples(out, max_rows); });
+}
+
+int fdf_mlp_init(fdf_handle* h, unsigned long long seed) {
+    return guarded(h, [&](fdf::Solver& s) {
+        s.synchronize();
+        fdf::mlp_init(s.mlp(), seed, s.stream());
+        s.refresh_stz();
+    });
+}
+
+int fdf_mlp_set_params(fdf_handle* h, const float* params) {
+    if (!params) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) {
+        s.synchronize();
+        fdf::mlp_set_params(s.mlp(), params, s.stream());
+        s.refresh_stz();
+    });
+}
+
+int fdf_mlp_get_params(fdf_handle* h, float* params) {
+    if (!params) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { fdf::mlp_get_params(s.mlp(), params, s.stream()); });
+}
+
+int fdf_mlp_infer(fdf_handle* h, const float* x, long long n, float* y, int force_thread) {
+    if (n < 0 || (n > 0 && (!x || !y))) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { fdf::mlp_infer(s.mlp(), x, n, y, force_thread, s.stream()); });
+}
+
+int fdf_mlp_gradients(fdf_handle* h, const float* x, const float* t, long long n, float* grads, double* loss) {
+    if (!x || !t || !grads || !loss || n <= 0) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { fdf::mlp_gradients(s.mlp(), x, t, n, grads, loss, s.stream()); });
+}
+
+int fdf_mlp_train(fdf_handle* h, int epochs, int batch, float lr, unsigned long long seed, double* train_loss,
+                  double* val_loss) {
+    if (!train_loss || !val_loss) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) {
+        s.synchronize();
+        s.mlp_train_on_samples(epochs, batch, lr, seed, train_loss, val_loss);
+        s.refresh_stz();
+    });
+}
+
 const char* fdf_last_error(fdf_handle* h) {
     if (!h) return g_create_error.c_str();
     return h->err.c_str();

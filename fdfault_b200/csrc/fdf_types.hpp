@@ -52,6 +52,24 @@ struct PertDev {
     const double* xy;   // spatial shape per fault node
 };
 
+// learned STZ initial guess: BF16 weights (stored as raw 16-bit words) and FP32 biases
+struct MlpDev {
+    const unsigned short* w1;   // [64][16]
+    const unsigned short* w2;   // [64][64]
+    const unsigned short* w3;   // [8][64]
+    const float *b1, *b2, *b3;
+};
+
+// STZ Newton counters and solver-generated training samples (both optional)
+struct StzAux {
+    int learned;                       // 1: start Newton from the network's guess
+    MlpDev mlp;
+    unsigned long long* stats;         // [0] Newton solves, [1] iterations, [2] starts from the midpoint
+    float* samples;                    // [cap][8]: 6 inputs, target logit(s)/20, converged mu
+    unsigned long long* nsamples;
+    unsigned long long cap;
+};
+
 struct IfaceDev {
     int kind;        // 0 locked, 1 frictionless, 2 slipweak, 3 stz
     int direction;
@@ -71,6 +89,7 @@ struct IfaceDev {
     const double* par[9];
     const unsigned char* fin1;   // 1 where this interface finalises the minus-side node
     const unsigned char* fin2;
+    StzAux stz;
 };
 
 // per-stage scalars

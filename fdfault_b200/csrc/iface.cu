@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include "kernels.hpp"
+#include "mlp_dev.cuh"
 #include "stage_common.cuh"
 
 namespace fdf {
@@ -88,8 +89,9 @@ __device__ __forceinline__ double stz_func(double mu, const StzPar& p) {
 }
 __device__ __forceinline__ double stz_der(double mu, const StzPar& p) { return p.eta * stz_dvpldmu(mu, p) - p.snc; }
 
-// bracketed Newton with bisection fallback; returns a status bit on failure
-__device__ int solve_newton(double xmin, double xmax, const StzPar& p, double* out) {
+// bracketed Newton with bisection fallback; returns a status bit on failure and
+// the number of iterations taken in *iters
+__device__ int solve_newton(double xmin, double xmax, const StzPar& p, double* out, int* iters) {
     const int nmax = 100;
     const double tol = 2.e-16;
     double func, der, x, xl, xh, fh, dx, dxold, temp;
@@ -115,9 +117,13 @@ __device__ int solve_newton(double xmin, double xmax, const StzPar& p, double* o
             func = stz_func(x, p);
             if (++guard > 4096) {
                 *out = x;
+                *iters = guard;
                 return FDF_ERR_NEWTON;
             }
         }
+        *iters = guard;
+    } else {
+        *iters = 0;
     }
     x = 0.5 * (xh + xl);
     func = stz_func(x, p);
@@ -128,6 +134,7 @@ __device__ int solve_newton(double xmin, double xmax, const StzPar& p, double* o
     while (i < nmax) {
         if (der == 0.) {
             *out = x;
+            *iters += i;
             return FDF_ERR_ZERO_DERIV;
         }
         if ((((x - xh) * der - func) * ((x - xl) * der - func) > 0.) || fabs(2. * func) > fabs(dxold * der)) {
@@ -152,10 +159,125 @@ __device__ int solve_newton(double xmin, double xmax, const StzPar& p, double* o
         i++;
     }
     *out = x;
+    *iters += i;
     return (i == nmax) ? FDF_ERR_NEWTON : 0;
 }
 
+// The same bracketed iteration started from x0 (the learned guess) instead of
+// the bracket midpoint: the bracket [xmin, xmax] is first narrowed by the sign
+// of f(x0) (a guess where f overflows becomes the new upper end and the start
+// moves to the midpoint, as in the plain solve).  Returns FDF_ERR_NEWTON if it
+// does not converge; the caller then falls back to the plain solve.
+__device__ int solve_newton_from(double xmin, double xmax, double x0, const StzPar& p, double* out, int* iters) {
+    const int nmax = 100;
+    const double tol = 2.e-16;
+    double xl = xmin, xh = xmax, x = x0;
+    double func = stz_func(x, p);
+    int guard = 0;
+    while (isinf(func) || isnan(func)) {
+        xh = x;
+        x = 0.5 * (xl + xh);
+        func = stz_func(x, p);
+        if (++guard > 4096) {
+            *iters = guard;
+            *out = x;
+            return FDF_ERR_NEWTON;
+        }
+    }
+    if (func < 0.)
+        xl = x;
+    else
+        xh = x;
+    double der = stz_der(x, p);
+    double dx = fabs(xh - xl), dxold = dx, temp;
+    int i = 0;
+    while (i < nmax) {
+        if (der == 0.) break;
+        if ((((x - xh) * der - func) * ((x - xl) * der - func) > 0.) || fabs(2. * func) > fabs(dxold * der)) {
+            dxold = dx;
+            dx = 0.5 * (xh - xl);
+            x = xl + dx;
+            if (xl == x) break;
+        } else {
+            dxold = dx;
+            dx = func / der;
+            temp = x;
+            x = x - dx;
+            if (temp == x) break;
+        }
+        if (fabs(dx) < tol) break;
+        func = stz_func(x, p);
+        der = stz_der(x, p);
+        if (func < 0.)
+            xl = x;
+        else
+            xh = x;
+        i++;
+    }
+    *out = x;
+    *iters = guard + i;
+    return (i == nmax || der == 0.) ? FDF_ERR_NEWTON : 0;
+}
+
+__device__ inline void stz_par(const IfaceDev& I, double phi, double eta, double snc, long long ij, double t,
+                               StzPar& p) {
+    p.phi = phi;
+    p.eta = eta;
+    p.snc = snc;
+    p.chi = I.state[ij];
+    p.v0 = pert_sum(I, 0, ij, t);
+    p.f0 = pert_sum(I, 1, ij, t);
+    p.a = pert_sum(I, 2, ij, t);
+    p.muy = pert_sum(I, 3, ij, t);
+    if (I.param_file) {
+        p.v0 += I.par[0][ij];
+        p.f0 += I.par[1][ij];
+        p.a += I.par[2][ij];
+        p.muy += I.par[3][ij];
+    }
+}
+
+// counters and training samples of one STZ Newton solve
+__device__ inline void stz_record(const IfaceDev& I, const StzPar& p, double mu, int iters, bool midpoint, int st,
+                                  const float* x) {
+    if (I.stz.stats) {   // one atomic per counter per warp
+        const unsigned mask = __activemask();
+        const unsigned n = __popc(mask);
+        const unsigned it = __reduce_add_sync(mask, (unsigned)iters);
+        const unsigned mid = __reduce_add_sync(mask, midpoint ? 1u : 0u);
+        if ((threadIdx.x & 31) == __ffs(mask) - 1) {
+            atomicAdd(&I.stz.stats[0], (unsigned long long)n);
+            atomicAdd(&I.stz.stats[1], (unsigned long long)it);
+            if (mid) atomicAdd(&I.stz.stats[2], (unsigned long long)mid);
+        }
+    }
+    if (I.stz.samples && st == 0) {
+        float xs[MLP_IN];
+        bool ok = true;
+        if (x) {
+            for (int i = 0; i < MLP_IN; i++) xs[i] = x[i];
+        } else {
+            ok = stz_features(p.phi, p.snc, p.chi, p.eta, p.v0, p.f0, p.a, p.muy, xs);
+        }
+        const double mh = -p.phi / p.snc;
+        if (ok) {
+            const unsigned long long k = atomicAdd(I.stz.nsamples, 1ULL);
+            if (k < I.stz.cap) {
+                // target t = logit(s)/20 with s and 1 - s each taken from its own
+                // difference (both ends of the bracket resolved)
+                const double w = mh - p.muy;
+                const double lo = fmax((mu - p.muy) / w, 1e-16), hi = fmax((mh - mu) / w, 1e-16);
+                float* o = I.stz.samples + 8 * k;
+                for (int i = 0; i < MLP_IN; i++) o[i] = xs[i];
+                o[6] = (float)((log(lo) - log(hi)) / 20.);
+                o[7] = (float)mu;
+            }
+        }
+    }
+}
+
 // friction::solve_fs (frictionless / stz) and slipweak::solve_fs
+template <bool LEARN>
 __device__ int solve_fs(const IfaceDev& I, double phi, double eta, double snc, long long ij, double t, double* bv,
                         double* bs) {
     int st = 0;
@@ -183,7 +305,62 @@ __device__ int solve_fs(const IfaceDev& I, double phi, double eta, double snc, l
         }
         return 0;
     }
-    if (snc < 0.) {
+    if (LEARN && I.kind == 3) {
+        // learned start: every lane evaluates the network (a full warp on the
+        // tensor cores) before the per-node branches
+        StzPar p;
+        stz_par(I, phi, eta, snc, ij, t, p);
+        float x[MLP_IN];
+        const bool feat = (snc < 0.) && stz_features(phi, snc, p.chi, eta, p.v0, p.f0, p.a, p.muy, x);
+        if (!feat)
+            for (int i = 0; i < MLP_IN; i++) x[i] = 0.f;
+        float y;
+        const unsigned act = __activemask();
+        if (act == 0xffffffffu) {
+            __syncwarp();
+            y = mlp_eval_warp(I.stz.mlp, x);
+        } else {
+            y = mlp_eval_thread(I.stz.mlp, x);
+        }
+        double mu = 0.;
+        if (snc < 0.) {
+            const double mh = -phi / snc;
+            if (p.muy >= mh) {
+                mu = mh;
+            } else {
+                int iters = 0, s1 = FDF_ERR_NEWTON;
+                bool midpoint = true;
+                // the network predicts t = logit(s)/20, s = (mu - muy)/(mh - muy):
+                // roots of creeping nodes sit within 1e-7 of the bracket's upper
+                // end, of fast-slipping nodes near its lower end.  The start is
+                // mh - q (mh - muy) with q = 1 - s, formed without cancellation.
+                if (feat && isfinite(y)) {
+                    const double z = fmin(fmax(20. * (double)y, -36.), 36.);
+                    const double q = 1. / (1. + exp(z));
+                    const double x0 = fmin(fmax(mh - q * (mh - p.muy), p.muy), mh);
+                    s1 = solve_newton_from(p.muy, mh, x0, p, &mu, &iters);
+                    midpoint = s1 != 0;
+                }
+                if (s1 != 0) {   // the plain solve judges and replaces a failed start
+                    int it2 = 0;
+                    s1 = solve_newton(p.muy, mh, p, &mu, &it2);
+                    iters += it2;
+                }
+                st |= s1;
+                if (I.stz.stats || I.stz.samples) stz_record(I, p, mu, iters, midpoint, s1, feat ? x : nullptr);
+            }
+            if (mu * fabs(snc) > phi) {
+                *bv = 0.;
+                *bs = phi;
+            } else {
+                *bs = mu * fabs(snc);
+                *bv = (phi - *bs) / eta;
+            }
+        } else {
+            *bs = 0.;
+            *bv = phi / eta;
+        }
+    } else if (snc < 0.) {
         double mu = 0.;
         if (I.kind == 3) {
             StzPar p;
@@ -201,10 +378,14 @@ __device__ int solve_fs(const IfaceDev& I, double phi, double eta, double snc, l
                 p.a += I.par[2][ij];
                 p.muy += I.par[3][ij];
             }
-            if (p.muy >= -phi / snc)
+            if (p.muy >= -phi / snc) {
                 mu = -phi / snc;
-            else
-                st |= solve_newton(p.muy, -phi / snc, p, &mu);
+            } else {
+                int iters = 0;
+                const int s1 = solve_newton(p.muy, -phi / snc, p, &mu, &iters);
+                st |= s1;
+                if (I.stz.stats || I.stz.samples) stz_record(I, p, mu, iters, true, s1, nullptr);
+            }
         }
         if (mu * fabs(snc) > phi) {
             *bv = 0.;
@@ -332,7 +513,7 @@ __device__ __forceinline__ void finish_fault_node(const IfaceArgs<T>& a, const B
     for (int q = 0; q < nf; q++) a.Fn[q * cs + id] = fn[q];
 }
 
-template <typename T>
+template <typename T, bool LEARN>
 __global__ void __launch_bounds__(128) k_interface(IfaceArgs<T> a, IfaceDev I, BlockDev B1, BlockDev B2, StageArgs sa,
                                                    int no_sat) {
     const long long nn = (long long)I.n0 * I.n1;
@@ -432,7 +613,7 @@ __global__ void __launch_bounds__(128) k_interface(IfaceArgs<T> a, IfaceDev I, B
         const double phi3 = eta * (is13 / zs1 - iv13 + is23 / zs2 + iv23);
         const double phi = sqrt(phi2 * phi2 + phi3 * phi3);
         double bv, bs;
-        status |= solve_fs(I, phi, eta, snc, ij, t, &bv, &bs);
+        status |= solve_fs<LEARN>(I, phi, eta, snc, ij, t, &bv, &bs);
         double v2, v3;
         if (bv == 0.) {
             v2 = 0.;
@@ -592,7 +773,11 @@ template <typename T>
 void launch_interface(const IfaceArgs<T>& a, const IfaceDev& itf, const BlockDev& b1, const BlockDev& b2,
                       const StageArgs& sa, int no_sat, cudaStream_t s) {
     long long nn = (long long)itf.n0 * itf.n1;
-    k_interface<T><<<(unsigned)((nn + 127) / 128), 128, 0, s>>>(a, itf, b1, b2, sa, no_sat);
+    const unsigned nb = (unsigned)((nn + 127) / 128);
+    if (itf.kind == 3 && itf.stz.learned)
+        k_interface<T, true><<<nb, 128, 0, s>>>(a, itf, b1, b2, sa, no_sat);
+    else
+        k_interface<T, false><<<nb, 128, 0, s>>>(a, itf, b1, b2, sa, no_sat);
 }
 template void launch_interface<double>(const IfaceArgs<double>&, const IfaceDev&, const BlockDev&, const BlockDev&,
                                        const StageArgs&, int, cudaStream_t);

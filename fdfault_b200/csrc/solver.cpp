@@ -247,6 +247,10 @@ Solver::~Solver() {
     for (void* p : {F_[0], F_[1], DF_, FP_, M_, J_, (void*)M64_, (void*)J64_, (void*)X_, (void*)S_, (void*)ABS_,
                     (void*)scratch_})
         if (p) cudaFree(p);
+    mlp_free(mlp_);
+    if (stz_counts_) cudaFree(stz_counts_);
+    if (samples_) cudaFree(samples_);
+    if (nsamples_) cudaFree(nsamples_);
     for (auto e : ev_pool_) cudaEventDestroy(e);
     for (auto& pe : ev_pending_) {
         cudaEventDestroy(pe.second.first);
@@ -956,6 +960,84 @@ void Solver::get_field_noalloc(int comp, bool absolute, double* out) {
     else
         launch_fetch_component<float>(L_, (const float*)base, c, absolute && comp < L_.nfields, P_.s0, S_, buf, stream_);
     fetch_to(buf, (size_t)n * sizeof(double), out);
+}
+
+void Solver::update_stz_aux() {
+    for (auto& I : ifaces_) {
+        if (I.kind != 3) continue;
+        I.stz.learned = stz_learned_ ? 1 : 0;
+        I.stz.mlp = mlp_.ready ? mlp_.dev() : MlpDev{};
+        I.stz.stats = stz_counting_ ? stz_counts_ : nullptr;
+        I.stz.samples = samples_;
+        I.stz.nsamples = nsamples_;
+        I.stz.cap = sample_cap_;
+    }
+}
+
+void Solver::set_stz_learned(bool on) {
+    if (on && !mlp_.ready) throw std::invalid_argument("the learned start needs network parameters (init, set or train)");
+    synchronize();
+    stz_learned_ = on;
+    update_stz_aux();
+}
+
+void Solver::set_stz_counting(bool on) {
+    synchronize();
+    if (on && !stz_counts_) {
+        cuda_check(cudaMalloc(&stz_counts_, 3 * sizeof(unsigned long long)), "cudaMalloc stz counters");
+        cuda_check(cudaMemset(stz_counts_, 0, 3 * sizeof(unsigned long long)), "stz counters");
+    }
+    stz_counting_ = on;
+    update_stz_aux();
+}
+
+void Solver::read_stz_counts(long long out[3], bool reset) {
+    unsigned long long h[3] = {0, 0, 0};
+    if (stz_counts_) {
+        cuda_check(cudaMemcpyAsync(h, stz_counts_, sizeof(h), cudaMemcpyDeviceToHost, stream_), "stz counters");
+        if (reset) cuda_check(cudaMemsetAsync(stz_counts_, 0, sizeof(h), stream_), "stz counters");
+        synchronize();
+    }
+    for (int i = 0; i < 3; i++) out[i] = (long long)h[i];
+}
+
+void Solver::stz_collect(long long capacity) {
+    if (capacity < 0) throw std::invalid_argument("negative sample capacity");
+    synchronize();
+    if (samples_) cudaFree(samples_);
+    if (nsamples_) cudaFree(nsamples_);
+    samples_ = nullptr;
+    nsamples_ = nullptr;
+    sample_cap_ = 0;
+    if (capacity > 0) {
+        cuda_check(cudaMalloc(&samples_, (size_t)capacity * 8 * sizeof(float)), "cudaMalloc samples");
+        cuda_check(cudaMalloc(&nsamples_, sizeof(unsigned long long)), "cudaMalloc sample count");
+        cuda_check(cudaMemset(nsamples_, 0, sizeof(unsigned long long)), "sample count");
+        sample_cap_ = (unsigned long long)capacity;
+    }
+    update_stz_aux();
+}
+
+long long Solver::stz_samples(float* out, long long max) {
+    if (!nsamples_) return 0;
+    unsigned long long n = 0;
+    cuda_check(cudaMemcpyAsync(&n, nsamples_, sizeof(n), cudaMemcpyDeviceToHost, stream_), "sample count");
+    synchronize();
+    const long long have = (long long)std::min<unsigned long long>(n, sample_cap_);
+    const long long k = std::min(have, max);
+    if (out && k > 0) {
+        cuda_check(cudaMemcpyAsync(out, samples_, (size_t)k * 8 * sizeof(float), cudaMemcpyDeviceToHost, stream_),
+                   "samples");
+        synchronize();
+    }
+    return have;
+}
+
+void Solver::mlp_train_on_samples(int epochs, int batch, float lr, unsigned long long seed, double* tr,
+                                  double* va) {
+    const long long have = stz_samples(nullptr, 0);
+    mlp_train(mlp_, samples_, have, epochs, batch, lr, seed, tr, va, stream_);
+    update_stz_aux();
 }
 
 void Solver::set_field(int comp, const double* in) {

@@ -18,6 +18,7 @@
 #include "fdf_types.hpp"
 #include "input.hpp"
 #include "kernels.hpp"
+#include "mlp.hpp"
 
 namespace fdf {
 
@@ -54,6 +55,16 @@ class Solver {
     void get_fault(int iface, int which, double* out);
     void set_fault(int iface, int which, const double* in);
     long long fault_count(int iface, int which) const;
+
+    // STZ friction: learned Newton start, counters, solver-generated samples
+    void set_stz_learned(bool on);
+    void set_stz_counting(bool on);
+    void read_stz_counts(long long out[3], bool reset);
+    void stz_collect(long long capacity);            // 0 stops collecting and frees the buffer
+    long long stz_samples(float* out, long long max);  // copies min(count, max) rows of 8 floats
+    MlpState& mlp() { return mlp_; }
+    void refresh_stz() { synchronize(); update_stz_aux(); }   // after the network's buffers change
+    void mlp_train_on_samples(int epochs, int batch, float lr, unsigned long long seed, double* tr, double* va);
 
     void synchronize();
     int check_status();            // reads and clears the device status word
@@ -126,6 +137,14 @@ class Solver {
 
     std::vector<BlockDev> blocks_;
     std::vector<IfaceDev> ifaces_;
+    MlpState mlp_;
+    bool stz_learned_ = false;
+    unsigned long long* stz_counts_ = nullptr;   // device [3]
+    bool stz_counting_ = false;
+    float* samples_ = nullptr;                   // device [cap][8]
+    unsigned long long* nsamples_ = nullptr;
+    unsigned long long sample_cap_ = 0;
+    void update_stz_aux();
     std::unique_ptr<OutputList> out_;
 
     // profiling

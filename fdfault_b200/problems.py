@@ -304,3 +304,68 @@ def planar3d(nx: int = 401, ny: int = 201, nz: int = 201, h: float = 0.1, nt: in
     p.interfaces.append(itf)
     p.outputs = list(outputs)
     return p
+
+
+# STZ constants of the planar STZ workload: a, muy, c0, R, beta, chiw, v1 are not
+# given by the workload's description and are chosen here (v0 and the ranges
+# of f0 and chi0 are given).  With chi0 spread over [0.05, 0.1] the initial
+# slip rate at one stress spans a factor e^10; a = 0.03 keeps the fault
+# creeping (up to a few cm/s outside the nucleation patch, dm/s inside) where
+# smaller a (0.02) starts the chi0 = 0.1 nodes at tens of m/s and the run
+# diverges.
+# chiw = 0.2 keeps the steady-state effective temperature below chi0 for all
+# slip rates below v1, so every node strengthens as it slips: with larger chiw
+# (1.2) single grid nodes heat up, run away and the run diverges.
+STZ_V0 = 1.0e-6
+STZ_CONSTANTS = dict(a=0.03, muy=0.3, c0=500.0, R=1.0e-3, beta=1.0, chiw=0.2, v1=1.0e4)
+
+
+def stz3d(nx: int = 401, ny: int = 201, nz: int = 201, h: float = 0.1, nt: int = 1500,
+          name: str = "stz3d", datadir: str = "data/", workdir: str = ".", seed: int = 4321,
+          rkorder: int = 3, sbporder: int = 4, cfl: float = 0.3, f0_range: Tuple[float, float] = (0.5, 0.6),
+          chi0_range: Tuple[float, float] = (0.05, 0.1), region: Tuple[float, float] = (20.0, 15.0),
+          muy_barrier: float = 10000.0, nuc_half: float = 1.0, sn: float = -120.0, s2: float = 70.0,
+          nuc_dtau: float = 11.6, outputs: Sequence[Output] = ()) -> Problem:
+    """3D vertical strike-slip fault with STZ friction: the planar geometry of
+    ``planar3d`` (two blocks of nx*ny*nz nodes split in y) with per-node STZ
+    parameters drawn from a seeded uniform distribution: f0 in ``f0_range``
+    (STZ parameter file) and the initial effective temperature chi0 in
+    ``chi0_range`` (state file); v0 = 1e-6 m/s and the other STZ constants
+    are STZ_CONSTANTS.  Outside a central region of ``region`` km (along
+    strike, along dip) the jamming friction muy is raised by ``muy_barrier``,
+    which locks the fault edges without a Newton solve (muy above the
+    traction ratio takes the solver's locked branch) -- the counterpart of
+    ``planar3d``'s static-friction barrier.  Loads and nucleation patch as in
+    ``planar3d``."""
+    lx, ly, lz = (nx - 1) * h, (ny - 1) * h, (nz - 1) * h
+    p = Problem(name=name, ndim=3, mode=2, nx_block=([nx], [ny, ny], [nz]), datadir=datadir, nt=nt,
+                cfl=cfl, rkorder=rkorder, sbporder=sbporder)
+    p.blocks[(0, 0, 0)] = Block(RHO, LAM, G, (0.0, 0.0, 0.0), (lx, ly, lz),
+                                ["absorbing", "absorbing", "absorbing", "none", "absorbing", "free"])
+    p.blocks[(0, 1, 0)] = Block(RHO, LAM, G, (0.0, ly, 0.0), (lx, ly, lz),
+                                ["absorbing", "absorbing", "none", "absorbing", "absorbing", "free"])
+    itf = Interface("y", (0, 0, 0), (0, 1, 0), "stz")
+    xc, zc = 0.5 * lx, 0.5 * lz
+    itf.loads = [load("constant", 0.0, 0.0, 0.0, 0.0, 0.0, sn, s2, 0.0),
+                 load("boxcar", 0.0, xc, nuc_half, zc, nuc_half, 0.0, nuc_dtau, 0.0)]
+    c = STZ_CONSTANTS
+    itf.perts = [stzparam("constant", 0.0, 0.0, 0.0, 0.0, 0.0, STZ_V0, 0.0, c["a"], c["muy"], c["c0"], c["R"],
+                          c["beta"], c["chiw"], c["v1"])]
+    rng = np.random.default_rng(seed)
+    f0 = rng.uniform(f0_range[0], f0_range[1], (nx, nz))
+    chi0 = rng.uniform(chi0_range[0], chi0_range[1], (nx, nz))
+    xs = np.arange(nx) * h
+    zs = np.arange(nz) * h
+    inside = (np.abs(xs[:, None] - xc) <= 0.5 * region[0]) & (np.abs(zs[None, :] - zc) <= 0.5 * region[1])
+    muy = np.where(inside, 0.0, muy_barrier)
+    zero = np.zeros((nx, nz))
+    pfile = os.path.join(workdir, name + ".stzparam")
+    np.stack([zero, f0, zero, muy, zero, zero, zero, zero, zero]).astype("<f8").tofile(pfile)
+    sfile = os.path.join(workdir, name + ".state")
+    chi0.astype("<f8").tofile(sfile)
+    itf.paramfile = pfile
+    itf.statefile = sfile
+    itf.chi0 = 0.0
+    p.interfaces.append(itf)
+    p.outputs = list(outputs)
+    return p

@@ -69,6 +69,18 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fdf_profile_read.argtypes = [ctypes.c_void_p, c_int, dp, P(c_ll)]
     L.fdf_use_fast_kernel.argtypes = [ctypes.c_void_p, c_int, P(c_int)]
     L.fdf_bytes_per_node_stage.argtypes = [ctypes.c_void_p, P(c_ll)]
+    fp = P(ctypes.c_float)
+    L.fdf_stz_set_learned.argtypes = [ctypes.c_void_p, c_int]
+    L.fdf_stz_set_counting.argtypes = [ctypes.c_void_p, c_int]
+    L.fdf_stz_read_counts.argtypes = [ctypes.c_void_p, P(c_ll), c_int]
+    L.fdf_stz_collect.argtypes = [ctypes.c_void_p, c_ll]
+    L.fdf_stz_samples.argtypes = [ctypes.c_void_p, fp, c_ll, P(c_ll)]
+    L.fdf_mlp_init.argtypes = [ctypes.c_void_p, ctypes.c_ulonglong]
+    L.fdf_mlp_set_params.argtypes = [ctypes.c_void_p, fp]
+    L.fdf_mlp_get_params.argtypes = [ctypes.c_void_p, fp]
+    L.fdf_mlp_infer.argtypes = [ctypes.c_void_p, fp, c_ll, fp, c_int]
+    L.fdf_mlp_gradients.argtypes = [ctypes.c_void_p, fp, fp, c_ll, fp, dp]
+    L.fdf_mlp_train.argtypes = [ctypes.c_void_p, c_int, c_int, ctypes.c_float, ctypes.c_ulonglong, dp, dp]
     L.fdf_last_error.argtypes = [ctypes.c_void_p]
     L.fdf_last_error.restype = ctypes.c_char_p
     _lib = L
@@ -77,6 +89,13 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
 
 def _dptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+MLP_NPARAM = 4673   # W1[64][6], b1[64], W2[64][64], b2[64], W3[64], b3
 
 
 class Problem:
@@ -160,6 +179,66 @@ class Problem:
         ms, n = ctypes.c_double(), ctypes.c_longlong()
         self._check(self._L.fdf_profile_read(self._h, kernel, ctypes.byref(ms), ctypes.byref(n)))
         return ms.value, n.value
+
+    # --- STZ friction: learned Newton start ------------------------------
+    def stz_learned(self, on: bool) -> None:
+        self._check(self._L.fdf_stz_set_learned(self._h, int(on)))
+
+    def stz_counting(self, on: bool) -> None:
+        self._check(self._L.fdf_stz_set_counting(self._h, int(on)))
+
+    def stz_counts(self, reset: bool = True) -> Tuple[int, int, int]:
+        """(Newton solves, iterations, solves started at the bracket midpoint)."""
+        c = (ctypes.c_longlong * 3)()
+        self._check(self._L.fdf_stz_read_counts(self._h, c, int(reset)))
+        return c[0], c[1], c[2]
+
+    def stz_collect(self, capacity: int) -> None:
+        self._check(self._L.fdf_stz_collect(self._h, capacity))
+
+    def stz_samples(self, max_rows: Optional[int] = None) -> np.ndarray:
+        """Collected rows [n][8]: 6 network inputs, target t = logit(s)/20, converged mu."""
+        n = ctypes.c_longlong()
+        self._check(self._L.fdf_stz_samples(self._h, None, 0, ctypes.byref(n)))
+        k = n.value if max_rows is None else min(n.value, max_rows)
+        out = np.zeros((k, 8), dtype=np.float32)
+        if k:
+            self._check(self._L.fdf_stz_samples(self._h, _fptr(out), k, ctypes.byref(n)))
+        return out
+
+    def mlp_init(self, seed: int) -> None:
+        self._check(self._L.fdf_mlp_init(self._h, seed))
+
+    def mlp_set_params(self, p: np.ndarray) -> None:
+        a = np.ascontiguousarray(p, dtype=np.float32).reshape(-1)
+        assert a.size == MLP_NPARAM
+        self._check(self._L.fdf_mlp_set_params(self._h, _fptr(a)))
+
+    def mlp_params(self) -> np.ndarray:
+        out = np.empty(MLP_NPARAM, dtype=np.float32)
+        self._check(self._L.fdf_mlp_get_params(self._h, _fptr(out)))
+        return out
+
+    def mlp_infer(self, x: np.ndarray, force_thread: bool = False) -> np.ndarray:
+        a = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 6)
+        y = np.empty(a.shape[0], dtype=np.float32)
+        self._check(self._L.fdf_mlp_infer(self._h, _fptr(a), a.shape[0], _fptr(y), int(force_thread)))
+        return y
+
+    def mlp_gradients(self, x: np.ndarray, t: np.ndarray) -> Tuple[np.ndarray, float]:
+        a = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 6)
+        tt = np.ascontiguousarray(t, dtype=np.float32).reshape(-1)
+        g = np.empty(MLP_NPARAM, dtype=np.float32)
+        loss = ctypes.c_double()
+        self._check(self._L.fdf_mlp_gradients(self._h, _fptr(a), _fptr(tt), a.shape[0], _fptr(g),
+                                              ctypes.byref(loss)))
+        return g, loss.value
+
+    def mlp_train(self, epochs: int, batch: int = 8192, lr: float = 1e-3, seed: int = 0) -> Tuple[float, float]:
+        """Adam on the collected samples; returns (last-epoch training loss, held-out loss)."""
+        tr, va = ctypes.c_double(), ctypes.c_double()
+        self._check(self._L.fdf_mlp_train(self._h, epochs, batch, lr, seed, ctypes.byref(tr), ctypes.byref(va)))
+        return tr.value, va.value
 
     def use_fast_kernel(self, on: bool) -> bool:
         act = ctypes.c_int()

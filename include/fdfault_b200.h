@@ -138,6 +138,43 @@ int fdf_bytes_per_node_stage(fdf_handle* h, long long* bytes);
 
 /* Message of the last failed call on h (or of the last failed fdf_create when
  * h is null). */
+/* ---- STZ friction with a learned Newton initial guess (no counterpart in
+ * the reference, whose solve always starts at the bracket midpoint,
+ * src/utilities.cpp:89-179 called from src/stz.cpp:296-303).
+ *
+ * A 6 -> 64 -> 64 -> 1 ReLU network (BF16 weights and activations, FP32
+ * accumulation) predicts t = log(s/(1-s))/20, s = (mu - muy)/(phi/|sn| - muy),
+ * for every STZ fault node from the node's traction, normal stress, state
+ * and parameters; the
+ * bracketed Newton iteration starts at that mu and falls back to the plain
+ * midpoint start when the guess is outside the bracket or does not converge.
+ * Parameters are one flat FP32 vector of FDF_MLP_NPARAM values:
+ * W1[64][6], b1[64], W2[64][64], b2[64], W3[64], b3. */
+#define FDF_MLP_NPARAM 4673
+int fdf_stz_set_learned(fdf_handle* h, int on);
+/* counters of the Newton solves: [0] solves, [1] iterations, [2] solves that
+ * started at the bracket midpoint (plain, or a rejected guess) */
+int fdf_stz_set_counting(fdf_handle* h, int on);
+int fdf_stz_read_counts(fdf_handle* h, long long* counts, int reset);
+/* solver-generated training samples, one row of 8 floats per converged
+ * Newton solve: the 6 network inputs, the target t and the converged mu;
+ * capacity 0 stops collecting.  fdf_stz_samples copies min(count, max_rows)
+ * rows and returns the number collected (capped at the capacity).  The target
+ * column holds t = log(s/(1-s))/20. */
+int fdf_stz_collect(fdf_handle* h, long long capacity);
+int fdf_stz_samples(fdf_handle* h, float* out, long long max_rows, long long* count);
+int fdf_mlp_init(fdf_handle* h, unsigned long long seed);
+int fdf_mlp_set_params(fdf_handle* h, const float* params);
+int fdf_mlp_get_params(fdf_handle* h, float* params);
+/* network outputs y[n] for inputs x[n][6]; force_thread=1 uses the per-thread
+ * path instead of the tensor-core warp path */
+int fdf_mlp_infer(fdf_handle* h, const float* x, long long n, float* y, int force_thread);
+/* gradient of 0.5*mean((y - t)^2) with respect to the parameters */
+int fdf_mlp_gradients(fdf_handle* h, const float* x, const float* t, long long n, float* grads, double* loss);
+/* Adam training on the collected samples (a tenth held out) */
+int fdf_mlp_train(fdf_handle* h, int epochs, int batch, float lr, unsigned long long seed, double* train_loss,
+                  double* val_loss);
+
 const char* fdf_last_error(fdf_handle* h);
 
 #ifdef __cplusplus

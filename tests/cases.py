@@ -218,6 +218,12 @@ def c_p3_stz(tmp):
     return p
 
 
+def c_p3_stz_files(tmp):
+    """STZ with per-node f0 (parameter file) and chi0 (state file), the planar STZ workload's set-up."""
+    return P.stz3d(nx=25, ny=13, nz=15, h=0.25, nt=12, name="p3_stz_files", workdir=tmp, nuc_half=0.75,
+                   region=(4.0, 2.5))
+
+
 def c_p3_xfault(tmp):
     p = P.Problem(name="p3_xfault", ndim=3, nx_block=([13, 13], [15], [14]), nt=10)
     p.blocks[(0, 0, 0)] = P.Block(P.RHO, P.LAM, P.G, (0., 0., 0.), (3., 3.5, 3.25),
@@ -274,12 +280,12 @@ CASES: Dict[str, Callable] = {
     "m2_plastic": c_m2_plastic, "m2_plastic_tensor": c_m2_plastic_tensor, "m2_curve": c_m2_curve,
     "m3": c_m3, "m3_plastic": c_m3_plastic, "m2_stz": c_m2_stz, "m2_four_blocks": c_m2_four_blocks,
     "p3_sw": c_p3_sw, "p3_rk4": c_p3_rk4, "p3_plastic": c_p3_plastic, "p3_stz": c_p3_stz,
-    "p3_xfault": c_p3_xfault, "p3_zfault": c_p3_zfault,
+    "p3_xfault": c_p3_xfault, "p3_zfault": c_p3_zfault, "p3_stz_files": c_p3_stz_files,
 }
 
 # cases whose friction law calls exp/log inside the per-stage solve (STZ);
 # device and host libm differ in the last bit there
-LIBM_CASES = {"m2_stz", "p3_stz"}
+LIBM_CASES = {"m2_stz", "p3_stz", "p3_stz_files"}
 
 
 def fault_fields(prob: P.Problem, iface: int = 0):
