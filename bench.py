@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=0)
     ap.add_argument("--size", default="full", choices=["full", "profile"],
                     help="profile: 2x201x101x101 instance for ncu captures")
+    ap.add_argument("--config", default="planar", choices=["planar", "stz"],
+                    help="stz: planar STZ fault, plain vs learned Newton start (one GPU)")
     return ap.parse_args()
 
 
@@ -216,11 +218,88 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
+def run_stz(args, local):
+    """Planar STZ workload (two blocks of 401x201x201, per-node f0 and chi0):
+    samples from a plain run, GPU training of the initial-guess network, then
+    the same steps timed with the plain and with the learned Newton start,
+    each compared with the FP64 plain run."""
+    import torch
+
+    from fdfault_b200 import problems as P
+    from fdfault_b200 import solver as fs
+
+    torch.cuda.set_device(local)
+    size = WORKLOAD if args.size == "full" else PROFILE_WORKLOAD
+    ncollect, epochs = 24, 20
+    nrun = args.warmup + args.steps + 2
+    tmp = tempfile.mkdtemp(prefix="fdf_stz_")
+    prob = P.stz3d(nt=max(ncollect, nrun) + 2, name="stz3d", datadir=tmp + "/", workdir=tmp, **size)
+    infile = prob.write(os.path.join(tmp, "stz3d.in"))
+    with fs.Problem(infile, precision=fs.FP32, device=local) as p:
+        p.stz_collect(2_400_000)
+        p.step(ncollect)
+        cnt = p.stz_sample_count()
+        p.mlp_init(7)
+        t0 = time.perf_counter()
+        tr, va = p.mlp_train(epochs=epochs, batch=8192, lr=2e-3, seed=3)
+        p.synchronize()
+        train_s = time.perf_counter() - t0
+        params = p.mlp_params()
+    runs = {}
+    keys = (fs.U, fs.V, fs.S, fs.STATE)
+    for mode in ("plain", "learned"):
+        with fs.Problem(infile, precision=fs.FP32, device=local) as q:
+            q.mlp_set_params(params)
+            q.stz_learned(mode == "learned")
+            q.step(args.warmup)
+            q.synchronize()
+            q.profile(True)
+            ms = q.time_steps(args.steps)
+            if_ms, if_n = q.profile_read(1)
+            vol_ms, vol_n = q.profile_read(0)
+            q.profile(False)
+            q.stz_counting(True)
+            q.step(2)
+            solves, iters, mid = q.stz_counts()
+            runs[mode] = dict(ms_per_step=ms / args.steps, interface_ms_per_stage=if_ms / max(if_n, 1),
+                              volume_ms_per_launch=vol_ms / max(vol_n, 1), newton_solves=solves,
+                              newton_iterations_per_solve=iters / max(solves, 1), midpoint_starts=mid,
+                              fault={w: q.fault(0, w) for w in keys}, nodes=q.nxyz, nstages=q.nstages)
+    with fs.Problem(infile, precision=fs.FP64, device=local) as r:
+        r.step(nrun)
+        ref = {w: r.fault(0, w) for w in keys}
+
+    def rel(a, b):
+        nb = float(np.linalg.norm(b))
+        return float(np.linalg.norm(a - b)) / (nb if nb > 0 else 1.0)
+
+    names = {fs.U: "slip", fs.V: "slip_rate", fs.S: "shear_stress", fs.STATE: "state"}
+    for mode in runs:
+        runs[mode]["rel_l2_vs_fp64"] = {names[w]: rel(runs[mode]["fault"][w], ref[w]) for w in keys}
+    learned_vs_plain = {names[w]: rel(runs["learned"]["fault"][w], runs["plain"]["fault"][w]) for w in keys}
+    for mode in runs:
+        del runs[mode]["fault"]
+    nodes, nst = runs["plain"]["nodes"], runs["plain"]["nstages"]
+    out = {"metric": METRIC, "value": nodes * nst / (runs["learned"]["ms_per_step"] * 1e-3), "unit": "node-stage/s",
+           "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32 fields, f64 friction", "data": "synthetic",
+           "config": {"workload": "stz3d: 2 blocks %dx%dx%d, STZ per-node f0 and chi0, learned Newton start"
+                                  % (size["nx"], size["ny"], size["nz"]), "nodes": nodes},
+           "training": {"samples": cnt, "collected_over_steps": ncollect, "epochs": epochs, "seconds": train_s,
+                        "train_loss": tr, "heldout_loss": va},
+           "plain": runs["plain"], "learned": runs["learned"], "learned_vs_plain_rel_l2": learned_vs_plain}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        return
+    if args.config == "stz":
+        if rank == 0:
+            run_stz(args, local)
         return
     import torch
 

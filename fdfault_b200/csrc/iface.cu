@@ -311,15 +311,17 @@ __device__ int solve_fs(const IfaceDev& I, double phi, double eta, double snc, l
         StzPar p;
         stz_par(I, phi, eta, snc, ij, t, p);
         float x[MLP_IN];
-        const bool feat = (snc < 0.) && stz_features(phi, snc, p.chi, eta, p.v0, p.f0, p.a, p.muy, x);
+        // only nodes that reach the Newton solve need the network
+        const bool need = (snc < 0.) && (p.muy < -phi / snc);
+        const bool feat = need && stz_features(phi, snc, p.chi, eta, p.v0, p.f0, p.a, p.muy, x);
         if (!feat)
             for (int i = 0; i < MLP_IN; i++) x[i] = 0.f;
-        float y;
+        float y = 0.f;
         const unsigned act = __activemask();
         if (act == 0xffffffffu) {
             __syncwarp();
-            y = mlp_eval_warp(I.stz.mlp, x);
-        } else {
+            if (__any_sync(0xffffffffu, feat)) y = mlp_eval_warp(I.stz.mlp, x);
+        } else if (feat) {
             y = mlp_eval_thread(I.stz.mlp, x);
         }
         double mu = 0.;
@@ -335,8 +337,8 @@ __device__ int solve_fs(const IfaceDev& I, double phi, double eta, double snc, l
                 // end, of fast-slipping nodes near its lower end.  The start is
                 // mh - q (mh - muy) with q = 1 - s, formed without cancellation.
                 if (feat && isfinite(y)) {
-                    const double z = fmin(fmax(20. * (double)y, -36.), 36.);
-                    const double q = 1. / (1. + exp(z));
+                    const float z = fminf(fmaxf(20.f * y, -36.f), 36.f);
+                    const double q = (double)(1.f / (1.f + __expf(z)));
                     const double x0 = fmin(fmax(mh - q * (mh - p.muy), p.muy), mh);
                     s1 = solve_newton_from(p.muy, mh, x0, p, &mu, &iters);
                     midpoint = s1 != 0;
@@ -513,8 +515,9 @@ __device__ __forceinline__ void finish_fault_node(const IfaceArgs<T>& a, const B
     for (int q = 0; q < nf; q++) a.Fn[q * cs + id] = fn[q];
 }
 
+// at most 128 registers: four CTAs per SM, one wave over a 401 x 201 fault
 template <typename T, bool LEARN>
-__global__ void __launch_bounds__(128) k_interface(IfaceArgs<T> a, IfaceDev I, BlockDev B1, BlockDev B2, StageArgs sa,
+__global__ void __launch_bounds__(128, 4) k_interface(IfaceArgs<T> a, IfaceDev I, BlockDev B1, BlockDev B2, StageArgs sa,
                                                    int no_sat) {
     const long long nn = (long long)I.n0 * I.n1;
     long long ij = blockIdx.x * (long long)blockDim.x + threadIdx.x;

@@ -159,14 +159,17 @@ __device__ inline float mlp_eval_warp(const MlpDev& m, const float x[MLP_IN]) {
 // bracket midpoint).
 __device__ inline bool stz_features(double phi, double snc, double chi, double eta, double v0, double f0, double a,
                                     double muy, float x[MLP_IN]) {
-    const double asn = fabs(snc) > 1e-300 ? fabs(snc) : 1e-300;
-    const double q = log(eta * v0 / asn) - f0 - 1. / chi;
-    const double v[MLP_IN] = {phi / asn, muy, a / 0.02, (q + 40.) / 10., log(asn) / 5., (1. / chi) / 20.};
+    // inputs only steer the start of the solve: single precision is enough
+    const float asn = (float)fmax(fabs(snc), 1e-30);
+    const float la = __logf(asn);
+    const float q = __logf((float)(eta * v0)) - la - (float)f0 - (float)(1. / chi);
+    const float v[MLP_IN] = {(float)(phi / fabs(snc)), (float)muy, (float)(a / 0.02), (q + 40.f) / 10.f, la / 5.f,
+                             (float)(1. / chi) / 20.f};
     bool ok = true;
 #pragma unroll
     for (int i = 0; i < MLP_IN; i++) {
-        ok = ok && isfinite(v[i]) && fabs(v[i]) < 1e4;
-        x[i] = ok ? (float)v[i] : 0.f;
+        ok = ok && isfinite(v[i]) && fabsf(v[i]) < 1e4f;
+        x[i] = ok ? v[i] : 0.f;
     }
     if (!ok) {
 #pragma unroll

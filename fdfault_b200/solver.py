@@ -196,6 +196,11 @@ class Problem:
     def stz_collect(self, capacity: int) -> None:
         self._check(self._L.fdf_stz_collect(self._h, capacity))
 
+    def stz_sample_count(self) -> int:
+        n = ctypes.c_longlong()
+        self._check(self._L.fdf_stz_samples(self._h, None, 0, ctypes.byref(n)))
+        return n.value
+
     def stz_samples(self, max_rows: Optional[int] = None) -> np.ndarray:
         """Collected rows [n][8]: 6 network inputs, target t = logit(s)/20, converged mu."""
         n = ctypes.c_longlong()
