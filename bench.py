@@ -49,8 +49,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=0)
     ap.add_argument("--size", default="full", choices=["full", "profile"],
                     help="profile: 2x201x101x101 instance for ncu captures")
-    ap.add_argument("--config", default="planar", choices=["planar", "stz"],
-                    help="stz: planar STZ fault, plain vs learned Newton start (one GPU)")
+    ap.add_argument("--config", default="planar", choices=["planar", "stz", "mode2"],
+                    help="stz: planar STZ fault, plain vs learned Newton start; mode2: 2D mode-II "
+                         "rupture in FP64 (one GPU each)")
     return ap.parse_args()
 
 
@@ -291,15 +292,96 @@ def run_stz(args, local):
     print(json.dumps(out), flush=True)
 
 
+def run_mode2(args, local):
+    """2D plane-strain mode-II rupture in FP64 (two blocks of 401x201, RK3, 1000
+    steps in the reference's configuration): device time of --steps steps, the
+    same steps through the C-ABI from host memory, and the reference solver on
+    the host cores for a sample of the same problem."""
+    import torch
+
+    from fdfault_b200 import problems as P
+    from fdfault_b200 import solver as fs
+
+    torch.cuda.set_device(local)
+    tmp = tempfile.mkdtemp(prefix="fdf_mode2_")
+    nt = args.warmup + 2 * args.steps + 2
+    prob = P.mode2_rupture(nx=401, ny=201, h=0.1, nt=nt, name="mode2", datadir=tmp + "/")
+    infile = prob.write(os.path.join(tmp, "mode2.in"))
+    with fs.Problem(infile, precision=fs.FP64, device=local) as p:
+        nodes, nst = p.nxyz, p.nstages
+        p.step(args.warmup)
+        p.synchronize()
+        clocks = ClockSampler(local)
+        clocks.start()
+        ms = p.time_steps(args.steps)   # default path: pairs of steps replayed from a CUDA graph
+        clk = clocks.stop()
+        p.profile(True)   # per-kernel event times: a separate pass, launched kernel by kernel
+        p.step(min(args.steps, 20))
+        vol_ms, vol_n = p.profile_read(0)
+        if_ms, if_n = p.profile_read(1)
+        p.profile(False)
+        # end to end: the state starts from host memory; the fault arrays come back every step
+        state = [p.field(c) for c in range(p.nfields)]
+        t0 = time.perf_counter()
+        for c in range(p.nfields):
+            p.set_field(c, state[c])
+        for _ in range(args.steps):
+            p.step(1)
+            p.fault(0, fs.V)
+            p.fault(0, fs.S)
+        p.synchronize()
+        te = time.perf_counter() - t0
+    value = nodes * nst * args.steps / (ms * 1e-3)
+    bps = 200
+    out = {"metric": METRIC, "value": value, "unit": "node-stage/s", "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "mode2: 2 blocks 401x201, slip weakening, RK3, FP64", "nodes": nodes,
+                      "l2": "resident in L2 (32 MB per stage): not graded against HBM"},
+           "clocks": clk,
+           "e2e": {"value": nodes * nst * args.steps / te, "unit": "node-stage/s",
+                   "h2d_bytes_per_step": 8.0 * nodes * len(state) / args.steps,
+                   "d2h_bytes_per_step": 2 * 8 * 401},
+           "kernel_ms": {"volume_avg": vol_ms / max(vol_n, 1), "volume_launches": vol_n,
+                         "interface_avg_per_stage": if_ms / max(if_n, 1)},
+           "roofline": {"bound": "latency", "achieved_gbs": bps * nodes / (vol_ms / max(vol_n, 1) * 2e-3) / 1e9,
+                        "algorithmic_bytes_per_node_stage": bps}}
+    if not args.no_cpu_baseline:
+        nproc = cpu_workers()
+        runs = []
+        for r in range(nproc):
+            d = os.path.join(tmp, "cpu%d" % r)
+            os.makedirs(d, exist_ok=True)
+            pr = P.mode2_rupture(nx=401, ny=201, h=0.1, nt=60, name="mode2", datadir=d + "/")
+            runs.append((d, pr.write(os.path.join(d, "mode2.in"))))
+        import oracle
+        if os.path.exists(oracle.REF_BIN):
+            procs = []
+            for d, f in runs:
+                tf = os.path.join(d, "timing.txt")
+                procs.append((subprocess.Popen([oracle.REF_BIN, f], cwd=d, env=dict(os.environ, FDF_REF_TIMING=tf),
+                                               stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL), tf))
+            secs = []
+            for pp, tf in procs:
+                pp.wait()
+                with open(tf) as fh:
+                    secs.append(float(fh.read().split()[-1]))
+            out["cpu_baseline"] = {"value": nodes * 3 * 60 * nproc / max(secs), "unit": "node-stage/s",
+                                   "cores": nproc, "kind": "reference",
+                                   "sample": "%d concurrent single-process runs of the same problem, 60 RK3 steps "
+                                             "each; time-stepping loop only (%.1f s)" % (nproc, max(secs))}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
         return
-    if args.config == "stz":
+    if args.config in ("stz", "mode2"):
         if rank == 0:
-            run_stz(args, local)
+            (run_stz if args.config == "stz" else run_mode2)(args, local)
         return
     import torch
 
@@ -332,15 +414,17 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    p.profile(True)
-    ms = p.time_steps(args.steps)
-    vol_ms, vol_n = p.profile_read(0)
-    if_ms, if_n = p.profile_read(1)
-    p.profile(False)
+    ms = p.time_steps(args.steps)   # default path: pairs of steps replayed from a CUDA graph
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     clk = clocks.stop()
+    # per-kernel event times for the roofline: a separate pass, launched kernel by kernel
+    p.profile(True)
+    p.step(min(args.steps, 20))
+    vol_ms, vol_n = p.profile_read(0)
+    if_ms, if_n = p.profile_read(1)
+    p.profile(False)
     p.synchronize()   # raises if any kernel reported a solver status
     if dist:
         t = torch.tensor([ms], device="cuda")
@@ -388,7 +472,9 @@ def main():
                 "peak_source": peak_kind, "kernel": "volume_fast3d" if fast else "volume_exact",
                 "algorithmic_bytes_per_node_stage": bps,
                 "traffic": (traffic_pn * nodes / nblocks) if traffic_pn else None}
-    launches = args.steps * nstages * (nblocks + p.nifaces)
+    # per step: one volume launch per block and one interface launch per interface per
+    # stage, plus the graph's step-counter kernel; one counter reset per call
+    launches = args.steps * (nstages * (nblocks + p.nifaces) + 1) + 1
     out = {"metric": METRIC, "value": value, "unit": "node-stage/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32" if precision == fs.FP32 else "f64", "data": "synthetic",

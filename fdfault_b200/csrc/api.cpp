@@ -186,6 +186,10 @@ int fdf_profile_read(fdf_handle* h, int kernel, double* total_ms, long long* lau
     return guarded(h, [&](fdf::Solver& s) { s.profile_read(kernel, total_ms, launches); });
 }
 
+int fdf_use_graphs(fdf_handle* h, int on) {
+    return guarded(h, [&](fdf::Solver& s) { s.use_graphs(on != 0); });
+}
+
 int fdf_use_fast_kernel(fdf_handle* h, int on, int* active) {
     return guarded(h, [&](fdf::Solver& s) {
         s.use_fast_kernel(on != 0);

@@ -102,6 +102,10 @@ struct StageArgs {
     double tfront;           // time recorded by the front tracker after this step
     int front_on;
     double front_value;
+    // graph replay: when set, t and tfront come from this device step counter
+    // (t = step*dt + cst*dt, tfront = (step+1)*dt, the host's expressions)
+    const int* step_dev;
+    double cst;
 };
 
 enum Status : int {

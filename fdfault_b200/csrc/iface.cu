@@ -532,7 +532,13 @@ __global__ void __launch_bounds__(128, 4) k_interface(IfaceArgs<T> a, IfaceDev I
     const long long st[3] = {L.s0, L.s1, L.s2};
     const long long i1 = node_index(L, pos[0], pos[1], pos[2]);
     const long long i2 = i1 + st[D];
-    const double dt = sa.dt, t = sa.t;
+    const double dt = sa.dt;
+    double t = sa.t, tfront = sa.tfront;
+    if (sa.step_dev) {
+        const int sd = *sa.step_dev;
+        t = (double)sd * dt + sa.cst * dt;
+        tfront = (double)(sd + 1) * dt;
+    }
     const bool fric = I.kind >= 1;
     const bool plastic = sa.plastic != 0;
     const T* F = no_sat ? a.Fn : a.F;
@@ -731,7 +737,7 @@ __global__ void __launch_bounds__(128, 4) k_interface(IfaceArgs<T> a, IfaceDev I
     }
     // front::set_front after the step (front.cpp:103-125; the U field never records)
     if (fric && sa.front_on && sa.last && (no_sat || !plastic)) {
-        if (I.tfront[ij] < 0. && I.v[ij] >= sa.front_value) I.tfront[ij] = sa.tfront;
+        if (I.tfront[ij] < 0. && I.v[ij] >= sa.front_value) I.tfront[ij] = tfront;
     }
 }
 
@@ -771,6 +777,12 @@ __global__ void k_front(IfaceDev I, double t, double value) {
 }
 
 }  // namespace
+
+__global__ void k_step_advance(int* step) { *step += 1; }
+__global__ void k_set_step(int* step, int value) { *step = value; }
+
+void launch_step_advance(int* step, cudaStream_t s) { k_step_advance<<<1, 1, 0, s>>>(step); }
+void launch_set_step(int* step, int value, cudaStream_t s) { k_set_step<<<1, 1, 0, s>>>(step, value); }
 
 template <typename T>
 void launch_interface(const IfaceArgs<T>& a, const IfaceDev& itf, const BlockDev& b1, const BlockDev& b2,

@@ -80,5 +80,7 @@ void launch_fetch_component(const Layout& L, const T* F, int comp, int add_stres
 template <typename T>
 void launch_store_component(const Layout& L, T* F, int comp, const double* in, cudaStream_t s);
 void launch_front(const IfaceDev& itf, double t, double value, cudaStream_t s);
+void launch_step_advance(int* step, cudaStream_t s);
+void launch_set_step(int* step, int value, cudaStream_t s);
 
 }  // namespace fdf

@@ -247,6 +247,9 @@ Solver::~Solver() {
     for (void* p : {F_[0], F_[1], DF_, FP_, M_, J_, (void*)M64_, (void*)J64_, (void*)X_, (void*)S_, (void*)ABS_,
                     (void*)scratch_})
         if (p) cudaFree(p);
+    for (auto g : graph_exec_)
+        if (g) cudaGraphExecDestroy(g);
+    if (step_dev_) cudaFree(step_dev_);
     mlp_free(mlp_);
     if (stz_counts_) cudaFree(stz_counts_);
     if (samples_) cudaFree(samples_);
@@ -779,6 +782,8 @@ void Solver::stage_impl(double dt, int stage, double t, bool for_step) {
     sa.front_on = (for_step && P_.front_on && P_.front_field == "V") ? 1 : 0;
     sa.front_value = P_.front_value;
     sa.tfront = (double)(step_index_ + 1) * dt;
+    sa.step_dev = capturing_ ? step_dev_ : nullptr;
+    sa.cst = C_[stage];
     T* Fo = (T*)F_[cur_];
     T* Fn = (T*)F_[1 - cur_];
     VolumeArgs<T> va{};
@@ -854,6 +859,55 @@ void Solver::do_rk_stage(double dt, int stage, double t) {
 }
 
 void Solver::step(int nsteps) {
+    // whole pairs of steps replay the captured graph when nothing on the host
+    // has to happen between steps (no output units, no per-launch profiling)
+    if (graphs_ && !out_ && !profile_ && nsteps >= 2) {
+        step_graph(nsteps / 2);
+        nsteps %= 2;
+    }
+    step_launches(nsteps);
+}
+
+void Solver::step_graph(int npairs) {
+    if (graph_dirty_) {
+        for (auto& g : graph_exec_)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+        graph_dirty_ = false;
+    }
+    if (!step_dev_) cuda_check(cudaMalloc(&step_dev_, sizeof(int)), "cudaMalloc step counter");
+    // the graph bakes in which field buffer is read first: one graph per parity
+    cudaGraphExec_t& exec = graph_exec_[cur_];
+    if (!exec) {
+        // two steps: an even number of stages, so the field buffers end where they began
+        const int cur0 = cur_, idx0 = step_index_;
+        cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed), "begin capture");
+        capturing_ = true;
+        for (int n = 0; n < 2; n++) {
+            for (int st = 0; st < nstages_; st++) {
+                if (precision_ == 0)
+                    stage_impl<double>(dt_, st, 0., true);
+                else
+                    stage_impl<float>(dt_, st, 0., true);
+            }
+            launch_step_advance(step_dev_, stream_);
+        }
+        capturing_ = false;
+        cudaGraph_t g = nullptr;
+        cuda_check(cudaStreamEndCapture(stream_, &g), "end capture");
+        cuda_check(cudaGraphInstantiate(&exec, g, 0), "graph instantiate");
+        cudaGraphDestroy(g);
+        if (cur_ != cur0) throw std::runtime_error("graph capture left the field buffers swapped");
+        step_index_ = idx0;
+    }
+    launch_set_step(step_dev_, step_index_, stream_);
+    for (int n = 0; n < npairs; n++) cuda_check(cudaGraphLaunch(exec, stream_), "graph launch");
+    step_index_ += 2 * npairs;
+}
+
+void Solver::step_launches(int nsteps) {
     for (int n = 0; n < nsteps; n++) {
         for (int st = 0; st < nstages_; st++) {
             if (precision_ == 0)
@@ -963,6 +1017,7 @@ void Solver::get_field_noalloc(int comp, bool absolute, double* out) {
 }
 
 void Solver::update_stz_aux() {
+    graph_dirty_ = true;
     for (auto& I : ifaces_) {
         if (I.kind != 3) continue;
         I.stz.learned = stz_learned_ ? 1 : 0;

@@ -71,7 +71,13 @@ class Solver {
     float time_steps(int nsteps);  // device time of nsteps steps, ms (CUDA events on the solver stream)
     void set_profile(bool on);
     void profile_read(int kernel, double* total_ms, long long* launches);
-    void use_fast_kernel(bool on) { fast_ = on; }
+    void use_fast_kernel(bool on) {
+        fast_ = on;
+        graph_dirty_ = true;
+    }
+    // replay steps from a captured CUDA graph of two steps (default on)
+    void use_graphs(bool on) { graphs_ = on; }
+    bool graphs() const { return graphs_; }
     bool fast_kernel_active() const;
 
     const ProblemSpec& spec() const { return P_; }
@@ -145,6 +151,14 @@ class Solver {
     unsigned long long* nsamples_ = nullptr;
     unsigned long long sample_cap_ = 0;
     void update_stz_aux();
+    // CUDA graph of two steps, replayed by step() when no output is due
+    bool graphs_ = true;
+    bool graph_dirty_ = true;
+    bool capturing_ = false;
+    int* step_dev_ = nullptr;
+    cudaGraphExec_t graph_exec_[2] = {nullptr, nullptr};   // one per field-buffer parity
+    void step_launches(int nsteps);
+    void step_graph(int npairs);
     std::unique_ptr<OutputList> out_;
 
     // profiling

@@ -68,6 +68,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fdf_profile.argtypes = [ctypes.c_void_p, c_int]
     L.fdf_profile_read.argtypes = [ctypes.c_void_p, c_int, dp, P(c_ll)]
     L.fdf_use_fast_kernel.argtypes = [ctypes.c_void_p, c_int, P(c_int)]
+    L.fdf_use_graphs.argtypes = [ctypes.c_void_p, c_int]
     L.fdf_bytes_per_node_stage.argtypes = [ctypes.c_void_p, P(c_ll)]
     fp = P(ctypes.c_float)
     L.fdf_stz_set_learned.argtypes = [ctypes.c_void_p, c_int]
@@ -244,6 +245,10 @@ class Problem:
         tr, va = ctypes.c_double(), ctypes.c_double()
         self._check(self._L.fdf_mlp_train(self._h, epochs, batch, lr, seed, ctypes.byref(tr), ctypes.byref(va)))
         return tr.value, va.value
+
+    def use_graphs(self, on: bool) -> None:
+        """Replay pairs of steps from a captured CUDA graph (default on)."""
+        self._check(self._L.fdf_use_graphs(self._h, int(on)))
 
     def use_fast_kernel(self, on: bool) -> bool:
         act = ctypes.c_int()

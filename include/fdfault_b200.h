@@ -128,6 +128,12 @@ int fdf_time_steps(fdf_handle* h, int nsteps, double* ms);
 int fdf_profile(fdf_handle* h, int on);
 int fdf_profile_read(fdf_handle* h, int kernel, double* total_ms, long long* launches);
 
+/* fdf_step / fdf_solve / fdf_time_steps run whole pairs of steps by replaying
+ * one captured CUDA graph of two steps when no output unit is due and
+ * per-launch profiling is off (default on=1); results are identical to the
+ * launch-by-launch path (the stage time comes from a device step counter). */
+int fdf_use_graphs(fdf_handle* h, int on);
+
 /* Choose between the tiled FP32 volume kernel (default) and the
  * one-thread-per-node kernel for FP32 problems; active=1 if the tiled kernel
  * will run. */

@@ -1,0 +1,63 @@
+"""Stepping by CUDA-graph replay (pairs of steps, stage time from a device step
+counter) gives bit-identical fields, fault arrays and rupture times to
+launching every kernel from the host, for time-dependent loads (t0 > 0),
+slip-weakening time weakening, plasticity, STZ friction (plain and learned
+start) and the tiled FP32 kernel, with even and odd step counts."""
+
+import os
+
+import numpy as np
+import pytest
+
+from cases import build_case
+from fdfault_b200 import problems as P
+from fdfault_b200 import solver as fs
+
+pytestmark = pytest.mark.gpu
+
+
+def snapshot(p):
+    out = [p.field(c) for c in range(p.nfields)]
+    out += [p.fault(i, w) for i in range(p.nifaces) for w in (fs.U, fs.V, fs.S, fs.SN, fs.TFRONT)]
+    return out
+
+
+def run(infile, precision, graphs, chunks, setup=None):
+    with fs.Problem(infile, precision=precision) as p:
+        if setup:
+            setup(p)
+        p.use_graphs(graphs)
+        for n in chunks:
+            p.step(n)
+        p.synchronize()
+        return snapshot(p), p.step_index
+
+
+@pytest.mark.parametrize("name,precision", [("m2_perts", fs.FP64), ("m2_sw", fs.FP64), ("m2_plastic", fs.FP64),
+                                            ("p3_sw", fs.FP32), ("p3_stz_files", fs.FP64),
+                                            ("p3_stz_files", fs.FP32)])
+def test_graph_replay_is_bit_identical(tmp_path, name, precision):
+    prob = build_case(name, str(tmp_path))
+    infile = prob.write(os.path.join(str(tmp_path), prob.name + ".in"))
+    chunks = [5, 2, 1, 4]   # odd and even counts: pairs replayed, the rest launched
+    a, ia = run(infile, precision, False, chunks)
+    b, ib = run(infile, precision, True, chunks)
+    assert ia == ib == sum(chunks)
+    for k, (x, y) in enumerate(zip(a, b)):
+        assert np.array_equal(x, y, equal_nan=True), k
+
+
+def test_graph_replay_learned_stz(tmp_path):
+    tmp = str(tmp_path)
+    prob = P.stz3d(nx=25, ny=13, nz=37, h=0.25, nt=12, name="g_stz", datadir=tmp + "/", workdir=tmp,
+                   nuc_half=0.75, region=(4.0, 8.0))
+    infile = prob.write(os.path.join(tmp, "g_stz.in"))
+
+    def setup(p):
+        p.mlp_init(5)
+        p.stz_learned(True)
+
+    a, _ = run(infile, fs.FP32, False, [12], setup)
+    b, _ = run(infile, fs.FP32, True, [12], setup)
+    for k, (x, y) in enumerate(zip(a, b)):
+        assert np.array_equal(x, y, equal_nan=True), k
