@@ -49,9 +49,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=0)
     ap.add_argument("--size", default="full", choices=["full", "profile"],
                     help="profile: 2x201x101x101 instance for ncu captures")
-    ap.add_argument("--config", default="planar", choices=["planar", "stz", "mode2"],
+    ap.add_argument("--config", default="planar", choices=["planar", "stz", "mode2", "ensemble"],
                     help="stz: planar STZ fault, plain vs learned Newton start; mode2: 2D mode-II "
-                         "rupture in FP64 (one GPU each)")
+                         "rupture in FP64; ensemble: 256 2D ruptures of uneven sizes, batched")
+    ap.add_argument("--members", type=int, default=256, help="ensemble members (all ranks together)")
     return ap.parse_args()
 
 
@@ -373,11 +374,122 @@ def run_mode2(args, local):
     print(json.dumps(out), flush=True)
 
 
+def run_ensemble(args, rank, world, local):
+    """256 2D mode-II slip-weakening ruptures, blocks of 101x51 ... 801x401
+    nodes (log-uniform), per-member friction and nucleation: batched launches
+    replayed from CUDA graphs, tiles from the autotuner.  Members are split
+    across ranks (no collective); the aggregate is all members' node-stages
+    over the slowest rank's device time."""
+    import torch
+
+    from fdfault_b200 import problems as P
+    from fdfault_b200 import solver as fs
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    tune_steps = 2
+    nt = tune_steps * 6 + args.warmup + args.steps + 24
+    tmp = tempfile.mkdtemp(prefix="fdf_ens_%d_" % rank)
+    allfiles = P.ensemble_members(n=args.members, seed=2024, workdir=tmp, nt=nt)
+    files = allfiles[rank::world]
+    t0 = time.perf_counter()
+    ens = fs.Ensemble(files, device=local)
+    setup_s = time.perf_counter() - t0
+    threads, tile = ens.autotune(tune_steps)
+    ens.run(args.warmup)
+    per_step = ens.node_stages_per_step()
+    clocks = ClockSampler(local)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = ens.time_steps(args.steps)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    total = float(per_step * args.steps)
+    if dist:
+        t = torch.tensor([ms, total], device="cuda", dtype=torch.float64)
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        ms, total = float(mx[0].item()), float(t[1].item())
+    ens.check_status()
+    # the same members stepped one problem at a time through their own handles
+    nsingle = 8
+    t1 = time.perf_counter()
+    for i in range(ens.size):
+        ens.member(i).step(nsingle)
+    for i in range(ens.size):
+        ens.member(i).synchronize()
+    single_s = time.perf_counter() - t1
+    single_rate = per_step * nsingle / single_s
+    out = {"metric": METRIC, "value": total / (ms * 1e-3), "unit": "node-stage/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, f64 friction",
+           "data": "synthetic",
+           "config": {"workload": "ensemble: %d 2D mode-II ruptures, blocks 101x51..801x401 log-uniform"
+                                  % args.members, "members_per_rank": len(files),
+                      "node_stages_per_step": per_step, "parallelism": "members split across ranks" if world > 1
+                      else "single", "setup_s": setup_s, "autotuned": {"threads": threads, "tile": tile}},
+           "clocks": clk,
+           "one_problem_at_a_time": {"value": single_rate, "unit": "node-stage/s", "steps": nsingle,
+                                     "note": "rank 0's members stepped one after another through their own "
+                                             "handles (per-problem launches and graphs), wall clock"},
+           "gpu_launches": args.steps * (3 * 2 + 1)}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        nproc = cpu_workers()
+        procs = []
+        import oracle
+        sample = allfiles[:nproc]
+        secs = []
+        nodes_sample = 0
+        if os.path.exists(oracle.REF_BIN):
+            for f in sample:
+                d = os.path.dirname(f)
+                name = os.path.splitext(os.path.basename(f))[0]
+                src = open(f).read().split("\n")
+                src[3] = "20"   # [fdfault.problem] nt
+                g = os.path.join(d, name + "_cpu.in")
+                with open(g, "w") as fh:
+                    fh.write("\n".join(src))
+                tf = os.path.join(d, name + "_timing.txt")
+                procs.append((subprocess.Popen([oracle.REF_BIN, g], cwd=d, env=dict(os.environ, FDF_REF_TIMING=tf),
+                                               stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL), tf))
+            for pp, tf in procs:
+                pp.wait()
+                with open(tf) as fh:
+                    secs.append(float(fh.read().split()[-1]))
+            for f in sample:
+                src = open(f).read().split("\n")
+                nxs = [int(v) for v in src[src.index("[fdfault.domain]") + 3].split()]
+                nodes_sample += nxs[0] * nxs[1] * nxs[2]
+            out["cpu_baseline"] = {"value": nodes_sample * 3 * 20 / max(secs), "unit": "node-stage/s", "cores": nproc,
+                                   "kind": "reference",
+                                   "sample": "the first %d members run concurrently by the reference solver, one "
+                                             "process each, 20 RK3 steps; time-stepping loop only (%.1f s)"
+                                             % (nproc, max(secs))}
+    ens.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        return
+    if args.config == "ensemble":
+        run_ensemble(args, rank, world, local)
         return
     if args.config in ("stz", "mode2"):
         if rank == 0:

@@ -7,10 +7,17 @@
 #include <stdexcept>
 #include <string>
 
+#include "ensemble.hpp"
 #include "solver.hpp"
 
 struct fdf_handle {
     fdf::Solver* s = nullptr;
+    std::string err;
+    bool borrowed = false;   // a member of an ensemble: the ensemble owns the solver
+};
+
+struct fdf_ensemble {
+    fdf::Ensemble* e = nullptr;
     std::string err;
 };
 
@@ -31,6 +38,21 @@ int guarded(fdf_handle* h, F&& f) {
         return FDF_ERR_ARG;
     }
 }
+
+template <typename F>
+int eguarded(fdf_ensemble* h, F&& f) {
+    if (!h || !h->e) return FDF_ERR_ARG;
+    try {
+        f(*h->e);
+        return 0;
+    } catch (const std::exception& e) {
+        h->err = e.what();
+        if (h->err.find("solver status") != std::string::npos) return FDF_ERR_SOLVER;
+        if (h->err.find("CUDA") != std::string::npos || h->err.find("cuda") != std::string::npos) return FDF_ERR_CUDA;
+        return FDF_ERR_ARG;
+    }
+}
+
 
 }  // namespace
 
@@ -60,7 +82,7 @@ int fdf_create(const char* infile, int precision, int device, fdf_handle** out) 
 void fdf_destroy(fdf_handle* h) {
     if (!h) return;
     try {
-        delete h->s;
+        if (!h->borrowed) delete h->s;
     } catch (...) {
     }
     delete h;
@@ -264,6 +286,102 @@ int fdf_mlp_train(fdf_handle* h, int epochs, int batch, float lr, unsigned long 
         s.mlp_train_on_samples(epochs, batch, lr, seed, train_loss, val_loss);
         s.refresh_stz();
     });
+}
+
+int fdf_ensemble_create(const char* const* infiles, int n, int device, fdf_ensemble** out) {
+    if (!infiles || n <= 0 || !out) return FDF_ERR_ARG;
+    *out = nullptr;
+    try {
+        std::vector<std::string> files;
+        for (int i = 0; i < n; i++) {
+            if (!infiles[i]) return FDF_ERR_ARG;
+            files.emplace_back(infiles[i]);
+        }
+        fdf_ensemble* h = new fdf_ensemble;
+        try {
+            h->e = new fdf::Ensemble(files, device);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+        return 0;
+    } catch (const std::exception& e) {
+        g_create_error = e.what();
+        std::string m = g_create_error;
+        if (m.find("CUDA") != std::string::npos || m.find("cuda") != std::string::npos) return FDF_ERR_CUDA;
+        return FDF_ERR_INPUT;
+    }
+}
+
+void fdf_ensemble_destroy(fdf_ensemble* h) {
+    if (!h) return;
+    try {
+        delete h->e;
+    } catch (...) {
+    }
+    delete h;
+}
+
+int fdf_ensemble_size(fdf_ensemble* h, int* n) {
+    if (!n) return FDF_ERR_ARG;
+    return eguarded(h, [&](fdf::Ensemble& e) { *n = e.size(); });
+}
+
+int fdf_ensemble_member(fdf_ensemble* h, int member, fdf_handle** out) {
+    if (!out) return FDF_ERR_ARG;
+    return eguarded(h, [&](fdf::Ensemble& e) {
+        fdf::Solver& s = e.member(member);
+        fdf_handle* m = new fdf_handle;
+        m->s = &s;
+        m->borrowed = true;
+        *out = m;
+    });
+}
+
+int fdf_ensemble_run(fdf_ensemble* h, int nsteps) {
+    if (nsteps < 0) return FDF_ERR_ARG;
+    return eguarded(h, [&](fdf::Ensemble& e) { e.run(nsteps); });
+}
+
+int fdf_ensemble_time_steps(fdf_ensemble* h, int nsteps, double* ms) {
+    if (nsteps < 0 || !ms) return FDF_ERR_ARG;
+    return eguarded(h, [&](fdf::Ensemble& e) { *ms = e.time_steps(nsteps); });
+}
+
+int fdf_ensemble_autotune(fdf_ensemble* h, int steps, int* threads, long long* tile) {
+    return eguarded(h, [&](fdf::Ensemble& e) {
+        const fdf::EnsConfig c = e.autotune(steps);
+        if (threads) *threads = c.threads;
+        if (tile) *tile = c.tile;
+    });
+}
+
+int fdf_ensemble_set_config(fdf_ensemble* h, int threads, long long tile) {
+    return eguarded(h, [&](fdf::Ensemble& e) {
+        fdf::EnsConfig c;
+        c.threads = threads;
+        c.tile = tile;
+        e.set_config(c);
+    });
+}
+
+int fdf_ensemble_use_graph(fdf_ensemble* h, int on) {
+    return eguarded(h, [&](fdf::Ensemble& e) { e.use_graph(on != 0); });
+}
+
+int fdf_ensemble_node_stages(fdf_ensemble* h, long long* per_step) {
+    if (!per_step) return FDF_ERR_ARG;
+    return eguarded(h, [&](fdf::Ensemble& e) { *per_step = e.node_stages_per_step(); });
+}
+
+int fdf_ensemble_check_status(fdf_ensemble* h) {
+    return eguarded(h, [&](fdf::Ensemble& e) { e.check_status(); });
+}
+
+const char* fdf_ensemble_last_error(fdf_ensemble* h) {
+    if (!h) return g_create_error.c_str();
+    return h->err.c_str();
 }
 
 const char* fdf_last_error(fdf_handle* h) {

@@ -99,6 +99,7 @@ class Solver {
 
   private:
     friend class OutputList;
+    friend class Ensemble;
     template <typename T>
     void stage_impl(double dt, int stage, double t, bool for_step);
     template <typename T>

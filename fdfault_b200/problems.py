@@ -369,3 +369,34 @@ def stz3d(nx: int = 401, ny: int = 201, nz: int = 201, h: float = 0.1, nt: int =
     p.interfaces.append(itf)
     p.outputs = list(outputs)
     return p
+
+
+def ensemble_members(n: int = 256, seed: int = 2024, workdir: str = ".", nt: int = 400,
+                     size_range: Tuple[Tuple[int, int], Tuple[int, int]] = ((101, 51), (801, 401)),
+                     h: float = 0.1) -> List[str]:
+    """``n`` 2D mode-II slip-weakening ruptures of uneven sizes, written as .in
+    files under ``workdir`` (returned in order).
+
+    Member i has two blocks of nx by ny nodes with nx drawn log-uniform in
+    the range of ``size_range`` (ny = nx // 2 + 1, so 101x51 ... 801x401) at a
+    common grid spacing ``h`` (so every member has the same time step and runs
+    ``nt`` steps); static and dynamic friction, slip-weakening distance and
+    the nucleation shear load are drawn uniformly per member: mus in [0.6,
+    0.75], mud in [0.45, 0.55], dc in [0.2, 0.6] m and the nucleation patch's
+    shear load 2 to 8 MPa above the static strength (mus * 120 MPa)."""
+    rng = np.random.default_rng(seed)
+    (lo, _), (hi, _) = size_range
+    files = []
+    for i in range(n):
+        nx = int(round(np.exp(rng.uniform(np.log(lo), np.log(hi)))))
+        ny = nx // 2 + 1
+        mus = float(rng.uniform(0.6, 0.75))
+        mud = float(rng.uniform(0.45, 0.55))
+        dc = float(rng.uniform(0.2, 0.6))
+        over = float(rng.uniform(2.0, 8.0))
+        nuc_dtau = mus * 120.0 + over - 70.0
+        name = "member%03d" % i
+        p = mode2_rupture(nx=nx, ny=ny, h=h, nt=nt, name=name, datadir=workdir.rstrip("/") + "/",
+                          mus=mus, mud=mud, dc=dc, nuc_dtau=nuc_dtau, nuc_half=min(1.5, 0.1 * (nx - 1) * h))
+        files.append(p.write(os.path.join(workdir, name + ".in")))
+    return files

@@ -16,7 +16,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from typing import Optional, Tuple
+from typing import Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -82,6 +82,21 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fdf_mlp_infer.argtypes = [ctypes.c_void_p, fp, c_ll, fp, c_int]
     L.fdf_mlp_gradients.argtypes = [ctypes.c_void_p, fp, fp, c_ll, fp, dp]
     L.fdf_mlp_train.argtypes = [ctypes.c_void_p, c_int, c_int, ctypes.c_float, ctypes.c_ulonglong, dp, dp]
+    vp = ctypes.c_void_p
+    L.fdf_ensemble_create.argtypes = [P(ctypes.c_char_p), c_int, c_int, P(vp)]
+    L.fdf_ensemble_destroy.argtypes = [vp]
+    L.fdf_ensemble_destroy.restype = None
+    L.fdf_ensemble_size.argtypes = [vp, P(c_int)]
+    L.fdf_ensemble_member.argtypes = [vp, c_int, P(vp)]
+    L.fdf_ensemble_run.argtypes = [vp, c_int]
+    L.fdf_ensemble_time_steps.argtypes = [vp, c_int, dp]
+    L.fdf_ensemble_autotune.argtypes = [vp, c_int, P(c_int), P(c_ll)]
+    L.fdf_ensemble_set_config.argtypes = [vp, c_int, c_ll]
+    L.fdf_ensemble_use_graph.argtypes = [vp, c_int]
+    L.fdf_ensemble_node_stages.argtypes = [vp, P(c_ll)]
+    L.fdf_ensemble_check_status.argtypes = [vp]
+    L.fdf_ensemble_last_error.argtypes = [vp]
+    L.fdf_ensemble_last_error.restype = ctypes.c_char_p
     L.fdf_last_error.argtypes = [ctypes.c_void_p]
     L.fdf_last_error.restype = ctypes.c_char_p
     _lib = L
@@ -102,13 +117,17 @@ MLP_NPARAM = 4673   # W1[64][6], b1[64], W2[64][64], b2[64], W3[64], b3
 class Problem:
     """One fdfault problem held on a GPU."""
 
-    def __init__(self, infile: str, precision: int = FP64, device: int = 0):
+    def __init__(self, infile: Optional[str], precision: int = FP64, device: int = 0, _handle=None, _owner=None):
         self._L = load_library()
-        h = ctypes.c_void_p()
-        rc = self._L.fdf_create(infile.encode(), precision, device, ctypes.byref(h))
-        if rc:
-            raise FdfaultError(self._L.fdf_last_error(None).decode())
+        if _handle is None:
+            h = ctypes.c_void_p()
+            rc = self._L.fdf_create(infile.encode(), precision, device, ctypes.byref(h))
+            if rc:
+                raise FdfaultError(self._L.fdf_last_error(None).decode())
+        else:
+            h = _handle   # a member of an Ensemble (which owns the solver)
         self._h = h
+        self._owner = _owner
         self.precision = precision
         ints = (ctypes.c_int * 16)()
         dbls = (ctypes.c_double * 3)()
@@ -309,3 +328,81 @@ class Problem:
         a = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
         assert a.size == self.fault_count(iface, which)
         self._check(self._L.fdf_set_fault(self._h, iface, which, _dptr(a)))
+
+
+class Ensemble:
+    """Independent FP32 problems advanced together by batched launches
+    (one volume and one interface launch per stage for all members, chunks
+    of steps replayed from a CUDA graph).  ``member(i)`` gives a Problem view
+    of member i for reading its fields and fault arrays."""
+
+    def __init__(self, infiles: Sequence[str], device: int = 0):
+        self._L = load_library()
+        arr = (ctypes.c_char_p * len(infiles))(*[f.encode() for f in infiles])
+        h = ctypes.c_void_p()
+        rc = self._L.fdf_ensemble_create(arr, len(infiles), device, ctypes.byref(h))
+        if rc:
+            raise FdfaultError(self._L.fdf_ensemble_last_error(None).decode())
+        self._h = h
+        self._members = {}
+        n = ctypes.c_int()
+        self._check(self._L.fdf_ensemble_size(self._h, ctypes.byref(n)))
+        self.size = n.value
+
+    def _check(self, rc: int) -> None:
+        if rc:
+            raise FdfaultError(self._L.fdf_ensemble_last_error(self._h).decode())
+
+    def member(self, i: int) -> Problem:
+        if i not in self._members:
+            h = ctypes.c_void_p()
+            self._check(self._L.fdf_ensemble_member(self._h, i, ctypes.byref(h)))
+            self._members[i] = Problem(None, FP32, _handle=h, _owner=self)
+        return self._members[i]
+
+    def run(self, nsteps: int) -> None:
+        self._check(self._L.fdf_ensemble_run(self._h, nsteps))
+
+    def time_steps(self, nsteps: int) -> float:
+        ms = ctypes.c_double()
+        self._check(self._L.fdf_ensemble_time_steps(self._h, nsteps, ctypes.byref(ms)))
+        return ms.value
+
+    def autotune(self, steps: int = 2) -> Tuple[int, int]:
+        th, tl = ctypes.c_int(), ctypes.c_longlong()
+        self._check(self._L.fdf_ensemble_autotune(self._h, steps, ctypes.byref(th), ctypes.byref(tl)))
+        return th.value, tl.value
+
+    def set_config(self, threads: int, tile: int) -> None:
+        self._check(self._L.fdf_ensemble_set_config(self._h, threads, tile))
+
+    def use_graph(self, on: bool) -> None:
+        self._check(self._L.fdf_ensemble_use_graph(self._h, int(on)))
+
+    def node_stages_per_step(self) -> int:
+        n = ctypes.c_longlong()
+        self._check(self._L.fdf_ensemble_node_stages(self._h, ctypes.byref(n)))
+        return n.value
+
+    def check_status(self) -> None:
+        self._check(self._L.fdf_ensemble_check_status(self._h))
+
+    def close(self) -> None:
+        for m in self._members.values():
+            m.close()
+        self._members = {}
+        if getattr(self, "_h", None):
+            self._L.fdf_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -181,6 +181,38 @@ int fdf_mlp_gradients(fdf_handle* h, const float* x, const float* t, long long n
 int fdf_mlp_train(fdf_handle* h, int epochs, int batch, float lr, unsigned long long seed, double* train_loss,
                   double* val_loss);
 
+/* ---- Batched ensemble of independent problems (no counterpart in the
+ * reference, which runs one problem per process).
+ *
+ * All members run in FP32 (fields) with FP64 friction, share the Runge-Kutta
+ * order, are elastic and use locked, frictionless or slip-weakening
+ * interfaces.  Each stage of all members is one batched volume launch and
+ * one batched interface launch over a work list of tiles; step counters and
+ * field-buffer parities live on the device, and chunks of 16 steps replay
+ * one captured CUDA graph.  A member's results are bit-identical to running
+ * it alone in FP32 with the one-thread-per-node volume kernel.  Members step
+ * min(nsteps, nt - step) steps. */
+typedef struct fdf_ensemble fdf_ensemble;
+int fdf_ensemble_create(const char* const* infiles, int n, int device, fdf_ensemble** out);
+void fdf_ensemble_destroy(fdf_ensemble* e);
+int fdf_ensemble_size(fdf_ensemble* e, int* n);
+/* a handle on member i for the per-problem read functions (fdf_get_field,
+ * fdf_get_fault, fdf_get_info ...); release it with fdf_destroy, which leaves
+ * the member to the ensemble.  Stepping it directly desynchronises it. */
+int fdf_ensemble_member(fdf_ensemble* e, int member, fdf_handle** out);
+int fdf_ensemble_run(fdf_ensemble* e, int nsteps);
+int fdf_ensemble_time_steps(fdf_ensemble* e, int nsteps, double* ms);
+/* times `steps` real steps with each candidate CTA size and tile size, keeps
+ * the fastest (tiling never changes results) */
+int fdf_ensemble_autotune(fdf_ensemble* e, int steps, int* threads, long long* tile);
+int fdf_ensemble_set_config(fdf_ensemble* e, int threads, long long tile);
+int fdf_ensemble_use_graph(fdf_ensemble* e, int on);
+/* sum over members of nodes x stages: node-stage updates per ensemble step */
+int fdf_ensemble_node_stages(fdf_ensemble* e, long long* per_step);
+/* reads and clears every member's status word; FDF_ERR_SOLVER if one is set */
+int fdf_ensemble_check_status(fdf_ensemble* e);
+const char* fdf_ensemble_last_error(fdf_ensemble* e);
+
 const char* fdf_last_error(fdf_handle* h);
 
 #ifdef __cplusplus
