@@ -397,7 +397,9 @@ def run_ensemble(args, rank, world, local):
     nt = tune_steps * 6 + args.warmup + args.steps + 24
     tmp = tempfile.mkdtemp(prefix="fdf_ens_%d_" % rank)
     allfiles = P.ensemble_members(n=args.members, seed=2024, workdir=tmp, nt=nt)
-    files = allfiles[rank::world]
+    from fdfault_b200 import replicas
+
+    files = replicas.partition(allfiles, rank, world)
     t0 = time.perf_counter()
     ens = fs.Ensemble(files, device=local)
     setup_s = time.perf_counter() - t0
@@ -412,13 +414,7 @@ def run_ensemble(args, rank, world, local):
     ms = ens.time_steps(args.steps)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    total = float(per_step * args.steps)
-    if dist:
-        t = torch.tensor([ms, total], device="cuda", dtype=torch.float64)
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        ms, total = float(mx[0].item()), float(t[1].item())
+    total, ms = replicas.reduce_totals(float(per_step * args.steps), ms, device="cuda")
     ens.check_status()
     # the same members stepped one problem at a time through their own handles
     nsingle = 8
@@ -538,11 +534,10 @@ def main():
     if_ms, if_n = p.profile_read(1)
     p.profile(False)
     p.synchronize()   # raises if any kernel reported a solver status
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    node_stages = nodes * nstages * args.steps * world
+    from fdfault_b200 import replicas
+
+    # replicas: every rank advances its own copy; work summed, time the slowest rank's
+    node_stages, ms = replicas.reduce_totals(float(nodes * nstages * args.steps), ms, device="cuda")
     value = node_stages / (ms * 1e-3)
 
     # end to end through the C-ABI with host buffers: upload the state from
@@ -568,11 +563,8 @@ def main():
             o.numpy()[:] = p.fault(0, w)
     p.synchronize()
     te = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([te], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        te = float(t.item())
-    e2e = nodes * nstages * ke * world / te
+    e2e_work, te = replicas.reduce_totals(float(nodes * nstages * ke), te, device="cuda")
+    e2e = e2e_work / te
 
     bps = p.bytes_per_node_stage()
     peak, peak_kind = measured_peak()
