@@ -91,14 +91,19 @@ int fdf_set_step(fdf_handle* h, int step);
  * output units see them. */
 int fdf_get_field(fdf_handle* h, int comp, int absolute, double* out);
 
-/* Same values as fdf_get_field, without any device allocation: the component
- * is gathered into one fixed static device buffer of FDF_NOALLOC_MAX_VALUES
- * doubles (8 MiB) per device, then copied to `out`.  No counterpart in the
- * reference (which has no device memory).  Fields larger than the buffer are
- * rejected with FDF_ERR_ARG.  The buffer is shared by every handle on the
- * device: calls that overlap in time (from several host threads, or on
- * several handles of one device) race on it and may return each other's
- * values; serialise them. */
+/* Same values as fdf_get_field, without any device allocation, for callers
+ * that may not allocate device memory once running (a service that sizes its
+ * GPU memory up front, or code under an external memory budget), whereas
+ * fdf_get_field may grow a scratch buffer with cudaMalloc.  The component is
+ * gathered into one fixed static device buffer of FDF_NOALLOC_MAX_VALUES
+ * doubles (8 MiB, held by every GPU that loads the library until exit), then
+ * copied to `out`.  No counterpart in the reference (which has no device
+ * memory).  Fields larger than the buffer are rejected with FDF_ERR_ARG.  The
+ * first call on a device looks up the buffer's device address (make it before
+ * any stream capture).  The buffer is shared by every handle on the device:
+ * calls that overlap on the GPU (from several host threads, or on several
+ * handles of one device) race on it and may return each other's values;
+ * serialise them. */
 #define FDF_NOALLOC_MAX_VALUES 1048576
 int fdf_get_field_noalloc(fdf_handle* h, int comp, int absolute, double* out);
 int fdf_set_field(fdf_handle* h, int comp, const double* in);

@@ -1,8 +1,11 @@
-"""fdf_get_field_noalloc (fixed static device buffer) returns exactly what
-fdf_get_field (growable scratch buffer) returns, on two calls in a row, for
-FP64 and FP32 problems, plain and absolute stress; fields larger than the buffer are
-rejected.  The file is collected last so the entry point is also exercised
-after every other GPU test has run."""
+"""fdf_get_field_noalloc -- the read-back for callers that may not allocate
+device memory once running (a service that sizes its GPU memory up front, or
+code under an external memory budget) -- gathers into one fixed static device
+buffer and returns exactly what fdf_get_field (growable scratch buffer)
+returns, on two calls in a row, for FP64 and FP32 problems, plain and
+absolute stress; fields larger than the buffer are rejected.  The file is
+collected last so the entry point is also exercised after every other GPU
+test has run."""
 
 import os
 import tempfile
