@@ -49,9 +49,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=0)
     ap.add_argument("--size", default="full", choices=["full", "profile"],
                     help="profile: 2x201x101x101 instance for ncu captures")
-    ap.add_argument("--config", default="planar", choices=["planar", "stz", "mode2", "ensemble"],
+    ap.add_argument("--config", default="planar", choices=["planar", "stz", "mode2", "ensemble", "rough"],
                     help="stz: planar STZ fault, plain vs learned Newton start; mode2: 2D mode-II "
-                         "rupture in FP64; ensemble: 256 2D ruptures of uneven sizes, batched")
+                         "rupture in FP64; ensemble: 256 2D ruptures of uneven sizes, batched; rough: "
+                         "rough fault with plasticity, two blocks of 601x301x301, FP32")
     ap.add_argument("--members", type=int, default=256, help="ensemble members (all ranks together)")
     return ap.parse_args()
 
@@ -61,6 +62,19 @@ def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return rank, world, local
+
+
+REF_TIMEOUT_S = 300   # a reference run in a CPU-baseline sample never holds the GPU longer than this
+
+
+def wait_bounded(proc, timeout=REF_TIMEOUT_S):
+    """Wait for a reference process; kill it and raise if it runs past `timeout` seconds."""
+    try:
+        proc.wait(timeout=timeout)
+    except subprocess.TimeoutExpired:
+        proc.kill()
+        proc.wait()
+        raise RuntimeError("reference sample ran longer than %d s" % timeout)
 
 
 def build_problem(workdir, nt, **size):
@@ -170,7 +184,7 @@ def cpu_reference_sample(workdir, nsteps, nproc):
                                            stderr=subprocess.DEVNULL), tf))
         secs = []
         for p, tf in procs:
-            p.wait()
+            wait_bounded(p)
             with open(tf) as fh:
                 secs.append(float(fh.read().split()[-1]))
     else:
@@ -179,7 +193,7 @@ def cpu_reference_sample(workdir, nsteps, nproc):
                 "t=time.perf_counter(); o.run(int(sys.argv[2])); print(time.perf_counter()-t)") % HERE
         procs = [subprocess.Popen([sys.executable, "-c", code, infile, str(nsteps)], stdout=subprocess.PIPE,
                                   text=True) for _, infile, _ in runs]
-        secs = [float(p.communicate()[0].split()[-1]) for p in procs]
+        secs = [float(p.communicate(timeout=REF_TIMEOUT_S)[0].split()[-1]) for p in procs]
     total = nodes * 3 * nsteps * nproc
     return total / max(secs), kind, nproc, max(secs)
 
@@ -364,7 +378,7 @@ def run_mode2(args, local):
                                                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL), tf))
             secs = []
             for pp, tf in procs:
-                pp.wait()
+                wait_bounded(pp)
                 with open(tf) as fh:
                     secs.append(float(fh.read().split()[-1]))
             out["cpu_baseline"] = {"value": nodes * 3 * 60 * nproc / max(secs), "unit": "node-stage/s",
@@ -458,7 +472,7 @@ def run_ensemble(args, rank, world, local):
                 procs.append((subprocess.Popen([oracle.REF_BIN, g], cwd=d, env=dict(os.environ, FDF_REF_TIMING=tf),
                                                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL), tf))
             for pp, tf in procs:
-                pp.wait()
+                wait_bounded(pp)
                 with open(tf) as fh:
                     secs.append(float(fh.read().split()[-1]))
             for f in sample:
@@ -478,6 +492,86 @@ def run_ensemble(args, rank, world, local):
         dist.destroy_process_group()
 
 
+def run_rough(args, local):
+    """Rough-fault rupture with Drucker-Prager plasticity and depth-dependent
+    stress, two blocks of 601x301x301 nodes (109 M), FP32 fields: device time
+    of --steps steps (graph replay), per-kernel times from a profiled pass,
+    and the reference solver on the host cores for a reduced instance."""
+    import torch
+
+    from fdfault_b200 import problems as P
+    from fdfault_b200 import solver as fs
+
+    torch.cuda.set_device(local)
+    size = dict(nx=601, ny=301, nz=301, h=0.1) if args.size == "full" else dict(nx=201, ny=101, nz=101, h=0.3)
+    tmp = tempfile.mkdtemp(prefix="fdf_rough_")
+    t0 = time.perf_counter()
+    prob = P.rough3d(nt=args.warmup + args.steps + 8, name="rough3d", datadir=tmp + "/", workdir=tmp, **size)
+    infile = prob.write(os.path.join(tmp, "rough3d.in"))
+    gen_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    p = fs.Problem(infile, precision=fs.FP32, device=local)
+    setup_s = time.perf_counter() - t0
+    fast = p.use_fast_kernel(True)
+    nodes, nst, nblocks = p.nxyz, p.nstages, int(np.prod(p.nblocks))
+    p.step(args.warmup)
+    p.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = p.time_steps(args.steps)
+    clk = clocks.stop()
+    p.profile(True)
+    p.step(min(args.steps, 6))
+    vol_ms, vol_n = p.profile_read(0)
+    if_ms, if_n = p.profile_read(1)
+    p.profile(False)
+    p.synchronize()
+    bps = p.bytes_per_node_stage()
+    vmax = float(np.max(p.fault(0, fs.V)))
+    p.close()
+    peak, peak_kind = measured_peak()
+    vol_avg = vol_ms / max(vol_n, 1)
+    achieved = bps * nodes / nblocks / (vol_avg * 1e-3) / 1e9
+    out = {"metric": METRIC, "value": nodes * nst * args.steps / (ms * 1e-3), "unit": "node-stage/s", "n_gpus": 1,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, f64 friction", "data": "synthetic",
+           "config": {"workload": "rough3d: 2 blocks %dx%dx%d, rough fault, Drucker-Prager plasticity, "
+                                  "depth-dependent stress" % (size["nx"], size["ny"], size["nz"]), "nodes": nodes,
+                      "generate_s": gen_s, "setup_s": setup_s, "max_slip_rate": vmax},
+           "clocks": clk,
+           "kernel_ms": {"volume_avg": vol_avg, "volume_launches": vol_n,
+                         "interface_avg_per_stage": if_ms / max(if_n, 1)},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "peak_source": peak_kind, "kernel": "volume_fast3d" if fast else "volume_exact",
+                        "algorithmic_bytes_per_node_stage": bps}}
+    if not args.no_cpu_baseline:
+        import oracle
+        if os.path.exists(oracle.REF_BIN):
+            nproc = min(cpu_workers(), 8)
+            procs, secs = [], []
+            # (at 121x61x61 the reference built here did not finish 3 steps in 500 s; 61x31x31 takes 1 s)
+            small = dict(nx=61, ny=31, nz=31, h=1.0)
+            for r in range(nproc):
+                d = os.path.join(tmp, "cpu%d" % r)
+                os.makedirs(d, exist_ok=True)
+                pr = P.rough3d(nt=3, name="rough_cpu", datadir=d + "/", workdir=d, **small)
+                f = pr.write(os.path.join(d, "rough_cpu.in"))
+                tf = os.path.join(d, "timing.txt")
+                procs.append((subprocess.Popen([oracle.REF_BIN, f], cwd=d, env=dict(os.environ, FDF_REF_TIMING=tf),
+                                               stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL), tf))
+            for pp, tf in procs:
+                wait_bounded(pp)
+                with open(tf) as fh:
+                    secs.append(float(fh.read().split()[-1]))
+            n_small = small["nx"] * 2 * small["ny"] * small["nz"]
+            out["cpu_baseline"] = {"value": n_small * 3 * 3 * nproc / max(secs), "unit": "node-stage/s",
+                                   "cores": nproc, "kind": "reference",
+                                   "sample": "%d concurrent single-process runs of the workload at 61x31x31 per "
+                                             "block, 3 RK3 steps each; time-stepping loop only (%.1f s)"
+                                             % (nproc, max(secs))}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -487,9 +581,9 @@ def main():
     if args.config == "ensemble":
         run_ensemble(args, rank, world, local)
         return
-    if args.config in ("stz", "mode2"):
+    if args.config in ("stz", "mode2", "rough"):
         if rank == 0:
-            (run_stz if args.config == "stz" else run_mode2)(args, local)
+            {"stz": run_stz, "mode2": run_mode2, "rough": run_rough}[args.config](args, local)
         return
     import torch
 

@@ -976,9 +976,17 @@ float Solver::time_steps(int nsteps) {
 }
 
 long long Solver::bytes_per_node_stage() const {
-    // read and write f and df once each, read the metric and Jacobian once
+    // read and write f and df once each, read the metric and Jacobian once;
+    // plastic problems once per step (on the last stage) also read and write
+    // the plastic fields and read the heterogeneous initial stress (FP64),
+    // counted here per stage, rounded down
     const int esz = precision_ == 0 ? 8 : 4;
-    return (long long)(4 * L_.nfields + L_.ndim * L_.ndim + 1) * esz;
+    long long b = (long long)(4 * L_.nfields + L_.ndim * L_.ndim + 1) * esz;
+    if (P_.plastic()) {
+        long long per_step = 2LL * L_.nfieldsp * esz + (S_ ? (long long)L_.ns * 8 : 0);
+        b += per_step / std::max(nstages_, 1);
+    }
+    return b;
 }
 
 void Solver::fetch_to(void* devbuf, size_t bytes, void* host) {

@@ -400,3 +400,106 @@ def ensemble_members(n: int = 256, seed: int = 2024, workdir: str = ".", nt: int
                           mus=mus, mud=mud, dc=dc, nuc_dtau=nuc_dtau, nuc_half=min(1.5, 0.1 * (nx - 1) * h))
         files.append(p.write(os.path.join(workdir, name + ".in")))
     return files
+
+
+def rough_surface(nx: int, nz: int, h: float, alpha: float = 1e-3, lmin: float = 0.2, lmax: float = 20.0,
+                  seed: int = 99) -> np.ndarray:
+    """Band-limited self-similar roughness r(x, z) in km on an nx by nz grid of spacing h.
+
+    Random Fourier phases from ``seed``, amplitude spectrum proportional to
+    |k|^-2 (power spectral density |k|^-4, the 2D self-similar case) for
+    wavelengths between ``lmin`` and ``lmax`` (and at least two grid
+    spacings), and root-mean-square height ``alpha`` times the longest
+    wavelength present (the domain length when that is shorter than lmax)."""
+    rng = np.random.default_rng(seed)
+    kx = np.fft.fftfreq(nx, d=h)
+    kz = np.fft.rfftfreq(nz, d=h)
+    kk = np.sqrt(kx[:, None] ** 2 + kz[None, :] ** 2)
+    lo = 1.0 / min(lmax, max((nx - 1) * h, (nz - 1) * h))
+    hi = 1.0 / max(lmin, 2.0 * h)
+    band = (kk >= lo) & (kk <= hi)
+    amp = np.where(band, 1.0 / np.maximum(kk, 1e-30) ** 2, 0.0)
+    phase = rng.uniform(0.0, 2.0 * np.pi, amp.shape)
+    surf = np.fft.irfft2(amp * np.exp(1j * phase), s=(nx, nz))
+    rms = float(np.sqrt(np.mean(surf ** 2)))
+    target = alpha / lo
+    return surf * (target / rms) if rms > 0 else surf
+
+
+def rough3d(nx: int = 601, ny: int = 301, nz: int = 301, h: float = 0.1, nt: int = 1000, name: str = "rough3d",
+            datadir: str = "data/", workdir: str = ".", seed: int = 99, alpha: float = 1e-3,
+            lmin: float = 0.2, lmax: float = 20.0, grad: float = 16.7, shear_ratio: float = 0.6,
+            cohesion: float = 5.0, friction: float = 0.6, tvisc: float = 0.01, nuc_half: float = 1.5,
+            nuc_dtau: float = 0.0, rkorder: int = 3, sbporder: int = 4, cfl: float = 0.3,
+            outputs: Sequence[Output] = ()) -> Problem:
+    """3D rough-fault rupture with Drucker-Prager plasticity.
+
+    Two blocks of nx*ny*nz nodes meet on a vertical fault y = ly + r(x, z),
+    r from ``rough_surface``; the side faces follow the fault edges so the
+    transfinite grids conform.  The free surface is the z+ face (depth
+    d = lz - z, km).  Initial volume stress (heterogeneous stress file):
+    sxx = syy = szz = -grad*d and sxy = shear_ratio*grad*d MPa, so the fault
+    normal stress is -grad*d MPa/km.  Plasticity: cohesion ``cohesion`` MPa,
+    internal friction ``friction``, viscosity ``tvisc`` * G (the viscoplastic
+    time times the shear modulus).  Slip-weakening friction (0.677, 0.525,
+    0.4 m) with a nucleation patch at mid-depth whose shear load is raised to
+    ``nuc_dtau`` MPa above the static strength there (0: just above it)."""
+    lx, ly, lz = (nx - 1) * h, (ny - 1) * h, (nz - 1) * h
+    p = Problem(name=name, ndim=3, mode=2, nx_block=([nx], [ny, ny], [nz]), datadir=datadir, nt=nt,
+                cfl=cfl, rkorder=rkorder, sbporder=sbporder)
+    p.material = "plastic"
+    xs = np.arange(nx) * h
+    zs = np.arange(nz) * h
+    r = rough_surface(nx, nz, h, alpha, lmin, lmax, seed)
+    yf = ly + r   # fault y(x, z)
+
+    def write(tag, arrs):
+        fn = os.path.join(workdir, "%s_%s.surf" % (name, tag))
+        np.stack(arrs).astype("<f8").tofile(fn)
+        return fn
+
+    X2, Z2 = np.meshgrid(xs, zs, indexing="ij")            # (nx, nz)
+    fault = write("fault", [X2, yf, Z2])
+    sides = {}
+    t = np.linspace(0.0, 1.0, ny)
+    for b, (y0, y1) in enumerate([(np.zeros_like(yf), yf), (yf, np.full_like(yf, 2 * ly))]):
+        # x faces: arrays over (y index, z)
+        xm = [np.zeros((ny, nz)), y0[0][None, :] + t[:, None] * (y1[0] - y0[0])[None, :], np.tile(zs, (ny, 1))]
+        xp = [np.full((ny, nz), lx), y0[-1][None, :] + t[:, None] * (y1[-1] - y0[-1])[None, :], np.tile(zs, (ny, 1))]
+        # z faces: arrays over (x, y index)
+        zm = [np.tile(xs[:, None], (1, ny)), y0[:, 0][:, None] + t[None, :] * (y1[:, 0] - y0[:, 0])[:, None],
+              np.zeros((nx, ny))]
+        zp = [np.tile(xs[:, None], (1, ny)), y0[:, -1][:, None] + t[None, :] * (y1[:, -1] - y0[:, -1])[:, None],
+              np.full((nx, ny), lz)]
+        youter = np.zeros_like(yf) if b == 0 else np.full_like(yf, 2 * ly)
+        outer = write("b%d_y%d" % (b, 0 if b == 0 else 1), [X2, youter, Z2])
+        ysurf = [outer, fault] if b == 0 else [fault, outer]
+        sides[b] = [write("b%d_x0" % b, xm), write("b%d_x1" % b, xp)] + ysurf + \
+                   [write("b%d_z0" % b, zm), write("b%d_z1" % b, zp)]
+    eta = tvisc * G
+    for b, key in enumerate([(0, 0, 0), (0, 1, 0)]):
+        bounds = ["absorbing", "absorbing", "absorbing", "none", "absorbing", "free"] if b == 0 else \
+                 ["absorbing", "absorbing", "none", "absorbing", "absorbing", "free"]
+        p.blocks[key] = Block(RHO, LAM, G, (0.0, b * ly, 0.0), (lx, ly, lz), bounds, surfaces=sides[b],
+                              plastic=(friction, cohesion, 0.0, eta))
+    # depth-dependent initial stress, node order (i, j, k) over the whole domain,
+    # written one x-plane at a time (the full-size file is several GB)
+    dplane = np.broadcast_to((lz - zs)[None, :], (2 * ny, nz))
+    planes = {"n": np.ascontiguousarray(-grad * dplane, dtype="<f8"),
+              "s": np.ascontiguousarray(shear_ratio * grad * dplane, dtype="<f8"),
+              "0": np.zeros((2 * ny, nz), dtype="<f8")}
+    sfile = os.path.join(workdir, name + ".stress")
+    with open(sfile, "wb") as fh:
+        for comp in "ns0n0n":   # sxx, sxy, sxz, syy, syz, szz
+            for _ in range(nx):
+                planes[comp].tofile(fh)
+    p.loadfile = sfile
+    itf = Interface("y", (0, 0, 0), (0, 1, 0), "slipweak")
+    xc, zc = 0.5 * lx, 0.5 * lz
+    dnuc = lz - zc
+    extra = (0.677 - shear_ratio) * grad * dnuc + nuc_dtau + 0.5
+    itf.loads = [load("boxcar", 0.0, xc, nuc_half, zc, nuc_half, 0.0, extra, 0.0)]
+    itf.perts = [swparam("constant", 0.0, 0.0, 0.0, 0.0, 0.0, 0.4, 0.677, 0.525)]
+    p.interfaces.append(itf)
+    p.outputs = list(outputs)
+    return p

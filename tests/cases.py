@@ -224,6 +224,12 @@ def c_p3_stz_files(tmp):
                    region=(4.0, 2.5))
 
 
+def c_p3_rough(tmp):
+    """Rough fault from surface files, Drucker-Prager plasticity, depth-dependent stress file
+    (the rough-fault workload's set-up at small size)."""
+    return P.rough3d(nx=25, ny=13, nz=15, h=0.25, nt=10, name="p3_rough", workdir=tmp, nuc_half=0.75)
+
+
 def c_p3_xfault(tmp):
     p = P.Problem(name="p3_xfault", ndim=3, nx_block=([13, 13], [15], [14]), nt=10)
     p.blocks[(0, 0, 0)] = P.Block(P.RHO, P.LAM, P.G, (0., 0., 0.), (3., 3.5, 3.25),
@@ -281,6 +287,7 @@ CASES: Dict[str, Callable] = {
     "m3": c_m3, "m3_plastic": c_m3_plastic, "m2_stz": c_m2_stz, "m2_four_blocks": c_m2_four_blocks,
     "p3_sw": c_p3_sw, "p3_rk4": c_p3_rk4, "p3_plastic": c_p3_plastic, "p3_stz": c_p3_stz,
     "p3_xfault": c_p3_xfault, "p3_zfault": c_p3_zfault, "p3_stz_files": c_p3_stz_files,
+    "p3_rough": c_p3_rough,
 }
 
 # cases whose friction law calls exp/log inside the per-stage solve (STZ);

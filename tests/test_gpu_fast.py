@@ -48,6 +48,9 @@ CASES = {
     # two tiles in j whose last tile overlaps the first (closure rows in both)
     "small_o4": lambda t: planar(t, "small_o4", nx=25, ny=13, nz=37, nt=12),
     "small_o3": lambda t: planar(t, "small_o3", nx=25, ny=13, nz=37, nt=12, sbporder=3),
+    # curvilinear rough fault from surface files, plasticity, depth-dependent stress file
+    "rough_plastic": lambda t: P.rough3d(nx=25, ny=13, nz=37, h=0.25, nt=10, name="rough_plastic",
+                                         datadir=t + "/", workdir=t, nuc_half=0.75),
 }
 
 
@@ -62,7 +65,7 @@ def stage_from_random_state(infile, fast, seed=21):
             p.set_rate(c, rng.uniform(-1e-3, 1e-3, p.nxyz))
         for stage in range(p.nstages):
             p.do_rk_stage(p.dt, stage, 0.0)
-            out.append({"f%d" % c: p.field(c) for c in range(p.nfields)})
+            out.append({"f%d" % c: p.field(c) for c in range(p.nfields + p.nfieldsp)})
             out[-1].update({"df%d" % c: p.rate(c) for c in range(p.nfields)})
     return active, out
 
