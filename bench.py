@@ -54,6 +54,8 @@ def parse():
                          "rupture in FP64; ensemble: 256 2D ruptures of uneven sizes, batched; rough: "
                          "rough fault with plasticity, two blocks of 601x301x301, FP32")
     ap.add_argument("--members", type=int, default=256, help="ensemble members (all ranks together)")
+    ap.add_argument("--volume-kernel", type=int, default=1, choices=[0, 1, 2],
+                    help="FP32 3D volume kernel: 0 reference order, 1 tiled (default), 2 staged (TMA)")
     return ap.parse_args()
 
 
@@ -512,7 +514,8 @@ def run_rough(args, local):
     t0 = time.perf_counter()
     p = fs.Problem(infile, precision=fs.FP32, device=local)
     setup_s = time.perf_counter() - t0
-    fast = p.use_fast_kernel(True)
+    vk = p.set_volume_kernel(args.volume_kernel)
+    fast = vk != 0
     nodes, nst, nblocks = p.nxyz, p.nstages, int(np.prod(p.nblocks))
     p.step(args.warmup)
     p.synchronize()
@@ -542,7 +545,7 @@ def run_rough(args, local):
            "kernel_ms": {"volume_avg": vol_avg, "volume_launches": vol_n,
                          "interface_avg_per_stage": if_ms / max(if_n, 1)},
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                        "peak_source": peak_kind, "kernel": "volume_fast3d" if fast else "volume_exact",
+                        "peak_source": peak_kind, "kernel": {0: "volume_exact", 1: "volume_tiled3d", 2: "volume_staged3d"}[vk],
                         "algorithmic_bytes_per_node_stage": bps}}
     if not args.no_cpu_baseline:
         import oracle
@@ -604,7 +607,8 @@ def main():
     t_setup = time.perf_counter()
     p = fs.Problem(infile, precision=precision, device=local)
     t_setup = time.perf_counter() - t_setup
-    fast = p.use_fast_kernel(True)
+    vk = p.set_volume_kernel(args.volume_kernel)
+    fast = vk != 0
     nodes = p.nxyz
     nstages = p.nstages
     nblocks = int(np.prod(p.nblocks))
@@ -667,7 +671,7 @@ def main():
     achieved = bytes_per_launch / (vol_avg_ms * 1e-3) / 1e9
     traffic_pn = profiled_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": peak_kind, "kernel": "volume_fast3d" if fast else "volume_exact",
+                "peak_source": peak_kind, "kernel": {0: "volume_exact", 1: "volume_tiled3d", 2: "volume_staged3d"}[vk],
                 "algorithmic_bytes_per_node_stage": bps,
                 "traffic": (traffic_pn * nodes / nblocks) if traffic_pn else None}
     # per step: one volume launch per block and one interface launch per interface per

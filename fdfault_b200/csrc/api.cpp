@@ -212,6 +212,14 @@ int fdf_use_graphs(fdf_handle* h, int on) {
     return guarded(h, [&](fdf::Solver& s) { s.use_graphs(on != 0); });
 }
 
+int fdf_set_volume_kernel(fdf_handle* h, int kind, int* active) {
+    if (kind < 0 || kind > 2) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) {
+        s.set_volume_kernel(kind);
+        if (active) *active = s.volume_kernel_active();
+    });
+}
+
 int fdf_use_fast_kernel(fdf_handle* h, int on, int* active) {
     return guarded(h, [&](fdf::Solver& s) {
         s.use_fast_kernel(on != 0);

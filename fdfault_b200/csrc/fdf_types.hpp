@@ -115,6 +115,7 @@ enum Status : int {
     FDF_ERR_MELT = 4,         // STZ slip rate above v1 (stz.cpp:341-344)
     FDF_ERR_NONFINITE = 8,    // NaN or Inf produced
     FDF_ERR_JACOBIAN = 16,    // non-positive Jacobian (block.cpp:1002)
+    FDF_ERR_TIMEOUT = 32,     // a bounded wait for staged data ran out (kernel returned early)
 };
 
 }  // namespace fdf

@@ -249,6 +249,7 @@ Solver::~Solver() {
         if (p) cudaFree(p);
     for (auto g : graph_exec_)
         if (g) cudaGraphExecDestroy(g);
+    free_staged_maps(staged_maps_);
     if (step_dev_) cudaFree(step_dev_);
     mlp_free(mlp_);
     if (stz_counts_) cudaFree(stz_counts_);
@@ -761,12 +762,16 @@ void Solver::profile_read(int kernel, double* total_ms, long long* launches) {
     *launches = prof_n_[kernel & 3];
 }
 
-bool Solver::fast_kernel_active() const {
-    if (!fast_ || precision_ != 1 || L_.ndim != 3) return false;
-    for (auto& B : blocks_)
-        if (!fast3d_supported(L_, B, P_.sbporder)) return false;
-    return true;
+int Solver::volume_kernel_active() const {
+    if (vkernel_ == 0 || precision_ != 1 || L_.ndim != 3) return 0;
+    for (auto& B : blocks_) {
+        if (vkernel_ == 1 && !fast3d_supported(L_, B, P_.sbporder)) return 0;
+        if (vkernel_ == 2 && !staged3d_supported(L_, B, P_.sbporder)) return 0;
+    }
+    return vkernel_;
 }
+
+bool Solver::fast_kernel_active() const { return volume_kernel_active() != 0; }
 
 template <typename T>
 void Solver::stage_impl(double dt, int stage, double t, bool for_step) {
@@ -800,7 +805,7 @@ void Solver::stage_impl(double dt, int stage, double t, bool for_step) {
     va.S = S_;
     va.ABS = (sa.roundtrip && sa.last) ? ABS_ : nullptr;
     va.plastic_tensor = P_.plastic_tensor ? 1 : 0;
-    const bool fast = fast_kernel_active();
+    const int vk = volume_kernel_active();
     for (size_t b = 0; b < blocks_.size(); b++) {
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (profile_) {
@@ -809,7 +814,13 @@ void Solver::stage_impl(double dt, int stage, double t, bool for_step) {
             cudaEventRecord(e0, stream_);
         }
         if constexpr (sizeof(T) == 4) {
-            if (fast)
+            if (vk == 2) {
+                if (!staged_maps_)
+                    staged_maps_ = make_staged_maps(L_, (const float*)F_[0], (const float*)F_[1], (const float*)M_,
+                                                    (const float*)J_, P_.sbporder);
+                launch_volume_staged3d(va, blocks_[b], sa, status_, staged_maps_, stream_);
+            }
+            else if (vk == 1)
                 launch_volume_fast3d(va, blocks_[b], sa, stream_);
             else
                 launch_volume_exact<T>(va, blocks_[b], sa, stream_);

@@ -71,10 +71,14 @@ class Solver {
     float time_steps(int nsteps);  // device time of nsteps steps, ms (CUDA events on the solver stream)
     void set_profile(bool on);
     void profile_read(int kernel, double* total_ms, long long* launches);
-    void use_fast_kernel(bool on) {
-        fast_ = on;
+    void use_fast_kernel(bool on) { set_volume_kernel(on ? 1 : 0); }
+    // FP32 3D volume kernel: 0 one thread per node (reference order), 1 tiled
+    // (per-thread global loads), 2 staged (bulk copies into shared memory)
+    void set_volume_kernel(int kind) {
+        vkernel_ = kind;
         graph_dirty_ = true;
     }
+    int volume_kernel_active() const;   // the kind that runs (0 when the chosen one does not apply)
     // replay steps from a captured CUDA graph of two steps (default on)
     void use_graphs(bool on) { graphs_ = on; }
     bool graphs() const { return graphs_; }
@@ -123,7 +127,8 @@ class Solver {
     int nt_ = 0, nstages_ = 0;
     double A_[5] = {0}, B_[5] = {0}, C_[6] = {0};
     int step_index_ = 0;
-    bool fast_ = true;
+    int vkernel_ = 1;
+    StagedMapsHost* staged_maps_ = nullptr;   // tensor maps of the FP32 arrays (staged kernel)
 
     // device buffers
     void* F_[2] = {nullptr, nullptr};

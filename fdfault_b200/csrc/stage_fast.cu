@@ -384,7 +384,17 @@ __global__ void __launch_bounds__(NT, MINB) k_fast3d(VolumeArgs<float> a, BlockD
                 if (!B.bactive[fc]) continue;
                 const int fa = (d == 0) ? j : i;
                 const int fb = (d == 2) ? j : k;
-                boundary_sat<float, 3, 2>(B, fc, fa, fb, (float)sa.dt, f, df, false);
+                // the SAT reads and writes through pointers: work on copies so that
+                // f and df stay in registers on every other node
+                float fl[9], dl[9];
+#pragma unroll
+                for (int c = 0; c < 9; c++) {
+                    fl[c] = f[c];
+                    dl[c] = df[c];
+                }
+                boundary_sat<float, 3, 2>(B, fc, fa, fb, (float)sa.dt, fl, dl, false);
+#pragma unroll
+                for (int c = 0; c < 9; c++) df[c] = dl[c];
             }
         }
         if (owner) {
@@ -395,8 +405,14 @@ __global__ void __launch_bounds__(NT, MINB) k_fast3d(VolumeArgs<float> a, BlockD
                 float fn[9];
 #pragma unroll
                 for (int c = 0; c < 9; c++) fn[c] = fmaf(Bcoef, df[c], f[c]);
-                if (sa.last && sa.plastic)
-                    finish_node<float>(L, B, sa, a.s0, a.S, nullptr, a.FP, a.plastic_tensor, id, fn, false);
+                if (sa.last && sa.plastic) {   // return map: indexes its copy by the layout
+                    float fl[9];
+#pragma unroll
+                    for (int c = 0; c < 9; c++) fl[c] = fn[c];
+                    finish_node<float>(L, B, sa, a.s0, a.S, nullptr, a.FP, a.plastic_tensor, id, fl, false);
+#pragma unroll
+                    for (int c = 0; c < 9; c++) fn[c] = fl[c];
+                }
 #pragma unroll
                 for (int c = 0; c < 9; c++) Fn[c * cs + id] = fn[c];
             }

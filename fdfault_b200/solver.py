@@ -68,6 +68,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fdf_profile.argtypes = [ctypes.c_void_p, c_int]
     L.fdf_profile_read.argtypes = [ctypes.c_void_p, c_int, dp, P(c_ll)]
     L.fdf_use_fast_kernel.argtypes = [ctypes.c_void_p, c_int, P(c_int)]
+    L.fdf_set_volume_kernel.argtypes = [ctypes.c_void_p, c_int, P(c_int)]
     L.fdf_use_graphs.argtypes = [ctypes.c_void_p, c_int]
     L.fdf_bytes_per_node_stage.argtypes = [ctypes.c_void_p, P(c_ll)]
     fp = P(ctypes.c_float)
@@ -268,6 +269,12 @@ class Problem:
     def use_graphs(self, on: bool) -> None:
         """Replay pairs of steps from a captured CUDA graph (default on)."""
         self._check(self._L.fdf_use_graphs(self._h, int(on)))
+
+    def set_volume_kernel(self, kind: int) -> int:
+        """FP32 3D volume kernel: 0 reference order, 1 tiled, 2 staged; returns the kind that runs."""
+        act = ctypes.c_int()
+        self._check(self._L.fdf_set_volume_kernel(self._h, kind, ctypes.byref(act)))
+        return act.value
 
     def use_fast_kernel(self, on: bool) -> bool:
         act = ctypes.c_int()

@@ -144,6 +144,12 @@ int fdf_use_graphs(fdf_handle* h, int on);
  * will run. */
 int fdf_use_fast_kernel(fdf_handle* h, int on, int* active);
 
+/* FP32 3D volume kernel by kind: 0 one thread per node (reference operation
+ * order), 1 tiled with per-thread global loads (the default), 2 staged (planes
+ * brought into shared memory by TMA tensor copies).  active = the kind that
+ * will run (0 where the chosen one does not apply to the problem). */
+int fdf_set_volume_kernel(fdf_handle* h, int kind, int* active);
+
 /* Algorithmic bytes moved per node per stage by the volume kernel. */
 int fdf_bytes_per_node_stage(fdf_handle* h, long long* bytes);
 

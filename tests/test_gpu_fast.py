@@ -54,12 +54,13 @@ CASES = {
 }
 
 
-def stage_from_random_state(infile, fast, seed=21):
-    """Fields and rates after each stage of one step from a seeded random state."""
+def stage_from_random_state(infile, kind, seed=21):
+    """Fields and rates after each stage of one step from a seeded random state,
+    with volume kernel `kind` (0 reference order, 1 tiled, 2 staged)."""
     rng = np.random.default_rng(seed)
     out = []
     with fs.Problem(infile, precision=fs.FP32) as p:
-        active = p.use_fast_kernel(fast)
+        active = p.set_volume_kernel(kind)
         for c in range(p.nfields):
             p.set_field(c, rng.uniform(-1, 1, p.nxyz))
             p.set_rate(c, rng.uniform(-1e-3, 1e-3, p.nxyz))
@@ -70,27 +71,30 @@ def stage_from_random_state(infile, fast, seed=21):
     return active, out
 
 
+@pytest.mark.parametrize("kind", [1, 2])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_fast_kernel_matches_reference_order_kernel(name, tmp_path):
-    """Same operator: one step from a random state agrees to FP32 rounding."""
+def test_fast_kernel_matches_reference_order_kernel(name, kind, tmp_path):
+    """Same operator: one step from a random state agrees to FP32 rounding
+    (tiled kernel, kind 1, and staged kernel, kind 2)."""
     prob = CASES[name](str(tmp_path))
     infile = prob.write(os.path.join(str(tmp_path), prob.name + ".in"))
-    act_fast, a = stage_from_random_state(infile, True)
-    act_slow, b = stage_from_random_state(infile, False)
-    assert act_fast and not act_slow
+    act_fast, a = stage_from_random_state(infile, kind)
+    act_slow, b = stage_from_random_state(infile, 0)
+    assert act_fast == kind and act_slow == 0
     for s in range(len(a)):
         for k in a[s]:
             e = rel_l2(a[s][k], b[s][k])
             assert e < 1e-5, (s, k, e)
 
 
+@pytest.mark.parametrize("kind", [1, 2])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_fast_kernel_rupture_close_to_fp64(name, tmp_path):
-    """A rupture run with the tiled kernel stays within the FP32 tolerance of the FP64 oracle."""
+def test_fast_kernel_rupture_close_to_fp64(name, kind, tmp_path):
+    """A rupture run with the tiled or staged kernel stays within the FP32 tolerance of the FP64 oracle."""
     prob = CASES[name](str(tmp_path))
     infile = prob.write(os.path.join(str(tmp_path), prob.name + ".in"))
     with fs.Problem(infile, precision=fs.FP32) as p:
-        assert p.use_fast_kernel(True)
+        assert p.set_volume_kernel(kind) == kind
         p.step(prob.nt)
         p.synchronize()
         v, f0 = p.fault(0, fs.V), p.field(0)
