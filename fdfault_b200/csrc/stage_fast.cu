@@ -16,13 +16,20 @@
 //    per SM overlap one CTA's loads with the other's arithmetic);
 //  * interior stencils are unrolled with immediate coefficients in the
 //    antisymmetric form c1 (u+1 - u-1) + c2 (u+2 - u-2) + c3 (u+3 - u-3);
-//    boundary closure rows use the tabulated rows;
-//  * the rate is accumulated in registers, the outer SAT added on face
-//    nodes, and f and df are written once.
+//    x and y closure rows (whole planes, whole warps) use the tabulated rows;
+//    in the two k-edge tiles of a block every lane evaluates one NTB-tap row
+//    whose weights and columns it set up once (interior lanes carry the
+//    centred row padded with zero weights), so no warp diverges on k;
+//  * the rate is accumulated in registers and written once; nodes on a block
+//    face are finished by a small second kernel (k_faces3d) that adds the
+//    outer SATs in face order and performs the RK update there, so the
+//    marching kernel carries no face code.
 // Momentum rates use sum_d (dt/rho/dx_d)/J * D_d(J m_d . sigma), which is
-// algebraically the reference's conservative form; stress rates use the
-// velocity-gradient form of the same non-conservative terms.  Arithmetic is
-// FP32 with FMA contraction; the FP64 exact-order kernel is stage_exact.cu.
+// algebraically the reference's conservative form; stress rates are formed
+// from the velocity gradient e_ab = sum_d (dt/dx_d) m_d,b D_d v_a as
+// lambda tr(e) delta_ab + G (e_ab + e_ba), algebraically the reference's
+// sum over directions of the same non-conservative terms.  Arithmetic is FP32
+// with FMA contraction; the FP64 exact-order kernel is stage_exact.cu.
 #include <cuda_runtime.h>
 
 
@@ -47,7 +54,9 @@ struct FastCfg {
     static constexpr int RING = R * 3 * NT;   // float2 entries
     static constexpr int TY = 3 * VH * TK;    // float2
     static constexpr int TZ = 3 * TJ * VW;    // float2
-    static constexpr size_t SMEM = sizeof(float2) * (RING + TY + TZ);
+    static constexpr int WROWS = 2 * NB + 1;  // k-edge weight rows: centred, left closure, right closure (negated)
+    static constexpr int WTAB = ((WROWS * NTB + 3) / 4) * 4;   // floats
+    static constexpr size_t SMEM = sizeof(float2) * (RING + TY + TZ) + sizeof(float) * WTAB;
 };
 
 // interior first-derivative weights in antisymmetric form (src/fd.cpp:53-83):
@@ -72,14 +81,15 @@ struct HaloNode {
     float s[6], v[3], m[3], J;
 };
 
-template <int ORDER, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_fast3d(VolumeArgs<float> a, BlockDev B, StageArgs sa, int chunk) {
+template <int ORDER, bool PLASTIC>
+__global__ void __launch_bounds__(NT, 2) k_fast3d(VolumeArgs<float> a, BlockDev B, StageArgs sa, int chunk) {
     using C = FastCfg<ORDER>;
     constexpr int H = C::H, R = C::R, NB = C::NB, NTB = C::NTB, VH = C::VH, VW = C::VW;
     extern __shared__ float2 smem2[];
     float2* ring = smem2;              // [R][3][NT]   (F_x,c , v_c)
     float2* ty = ring + C::RING;       // [3][VH][TK]  (F_y,c , v_c)
     float2* tz = ty + C::TY;           // [3][TJ][VW]  (F_z,c , v_c)
+    float* wtab = (float*)(tz + C::TZ);   // [WROWS][NTB]
 
     const Layout& L = a.L;
     const int cs = (int)L.cstride;
@@ -100,6 +110,32 @@ __global__ void __launch_bounds__(NT, MINB) k_fast3d(VolumeArgs<float> a, BlockD
     const int ib = blockIdx.z * chunk;
     const int ie = min(n0, ib + chunk);
     if (ib >= ie) return;
+
+    // k-edge tiles (first and last in k): one NTB-tap row per lane
+    const bool kedge = (blockIdx.x == 0) || lastk;
+    if (kedge && tid < C::WROWS * NTB) {
+        const int r = tid / NTB, n = tid % NTB;
+        float w;
+        if (r == 0)
+            w = (n <= 2 * H) ? sbp_coef<float>(ORDER, 0, n) : 0.f;
+        else if (r <= NB)
+            w = sbp_coef<float>(ORDER, r, n);
+        else
+            w = -sbp_coef<float>(ORDER, r - NB, n);
+        wtab[tid] = w;
+    }
+    // this lane's row: tap n reads column kb + ks * min(n, kmax) of its tz row
+    int kb = tk, ks = 1, kmax = 2 * H, kw = 0;
+    if (ownk && k < NB) {
+        kb = H - k0;
+        kmax = NTB - 1;
+        kw = (k + 1) * NTB;
+    } else if (ownk && k >= n2 - NB) {
+        kb = (n2 - 1 - k0) + H;
+        ks = -1;
+        kmax = NTB - 1;
+        kw = (NB + n2 - k) * NTB;
+    }
 
     const int s0 = (int)L.s0;
     const int colbase = B.lo[0] * s0 + (B.lo[1] + j) * (int)L.s1 + (B.lo[2] + k);
@@ -130,17 +166,16 @@ __global__ void __launch_bounds__(NT, MINB) k_fast3d(VolumeArgs<float> a, BlockD
     const int hbase = B.lo[0] * s0 + (B.lo[1] + j0 + hj) * (int)L.s1 + (B.lo[2] + k0 + hk);
     const int hrow = (hkind == 0) ? 3 : 6;   // metric row y or z
 
-    float crho[3], cg2l[3], cg[3], clam[3];
+    float crho[3], sd[3];
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         crho[d] = (float)B.coef[d][0];
-        cg2l[d] = (float)B.coef[d][1];
-        cg[d] = (float)B.coef[d][2];
-        clam[d] = (float)B.coef[d][3];
+        sd[d] = (float)(sa.dt / B.dx[d]);
     }
+    const float lamc = (float)B.lam, gc = (float)B.g, g2c = (float)(2. * B.g);
     const float Acoef = (float)sa.A, Bcoef = (float)sa.B;
     const bool jint = (j >= NB) && (j < n1 - NB);
-    const bool kint = (k >= NB) && (k < n2 - NB);
+    const bool face = (j == 0) | (j == n1 - 1) | (k == 0) | (k == n2 - 1);
 
     auto mintap = [&](int i) { return i < NB ? 0 : (i >= n0 - NB ? n0 - NTB : i - H); };
     auto maxtap = [&](int i) { return i < NB ? NTB - 1 : (i >= n0 - NB ? n0 - 1 : i + H); };
@@ -263,7 +298,6 @@ __global__ void __launch_bounds__(NT, MINB) k_fast3d(VolumeArgs<float> a, BlockD
         } else {
             const bool left = i < NB;
             const int row = left ? i + 1 : n0 - i;
-            const int base = left ? 0 : n0 - 1, step = left ? 1 : -1;
             const float sg = left ? 1.f : -1.f;
 #pragma unroll
             for (int c = 0; c < 3; c++) {
@@ -284,7 +318,6 @@ __global__ void __launch_bounds__(NT, MINB) k_fast3d(VolumeArgs<float> a, BlockD
         // have taps outside the tile: give them the interior form, whose taps
         // always lie in the tile and its halo, and discard the result
         const bool jskip = !jint && !ownj;
-        const bool kskip = !kint && !ownk;
         if (jint || jskip) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
@@ -317,7 +350,7 @@ __global__ void __launch_bounds__(NT, MINB) k_fast3d(VolumeArgs<float> a, BlockD
                 Dv[1][c] = sg * av;
             }
         }
-        if (kint || kskip) {
+        if (!kedge) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 float af = 0.f, av = 0.f;
@@ -332,80 +365,64 @@ __global__ void __launch_bounds__(NT, MINB) k_fast3d(VolumeArgs<float> a, BlockD
                 Dv[2][c] = av;
             }
         } else {
-            const bool left = k < NB;
-            const int row = left ? k + 1 : n2 - k;
-            const int base = (left ? 0 : n2 - 1) - k0 + H, step = left ? 1 : -1;
-            const float sg = left ? 1.f : -1.f;
+            float af[3] = {0.f, 0.f, 0.f}, av[3] = {0.f, 0.f, 0.f};
+            const float2* trow = tz + tj * VW;
+#pragma unroll
+            for (int n = 0; n < NTB; n++) {
+                const float w = wtab[kw + n];
+                const int col = kb + ks * min(n, kmax);
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const float2 p = trow[c * TJ * VW + col];
+                    af[c] = fmaf(w, p.x, af[c]);
+                    av[c] = fmaf(w, p.y, av[c]);
+                }
+            }
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                float af = 0.f, av = 0.f;
-                for (int n = 0; n < NTB; n++) {
-                    const float cf = sbp_coef<float>(ORDER, row, n);
-                    const float2 p = tz[(c * TJ + tj) * VW + base + n * step];
-                    af = fmaf(cf, p.x, af);
-                    av = fmaf(cf, p.y, av);
-                }
-                DFl[2][c] = sg * af;
-                Dv[2][c] = sg * av;
+                DFl[2][c] = af[c];
+                Dv[2][c] = av[c];
             }
         }
         __syncthreads();   // shared tiles are rewritten for the next plane
 
         // ---- rate: df = A df + L(f)
-#pragma unroll
-        for (int c = 0; c < 9; c++) df[c] *= Acoef;
         const float iJ = __frcp_rn(Jc);
+        {
+            const float w0 = crho[0] * iJ, w1 = crho[1] * iJ, w2 = crho[2] * iJ;
 #pragma unroll
-        for (int d = 0; d < 3; d++) {
-            const float w = crho[d] * iJ;
-            const float ma = m[3 * d], mb = m[3 * d + 1], mc = m[3 * d + 2];
-            df[0] = fmaf(w, DFl[d][0], df[0]);
-            df[1] = fmaf(w, DFl[d][1], df[1]);
-            df[2] = fmaf(w, DFl[d][2], df[2]);
-            const float dvx = Dv[d][0], dvy = Dv[d][1], dvz = Dv[d][2];
-            df[3] += cg2l[d] * ma * dvx + clam[d] * (mb * dvy + mc * dvz);
-            df[4] += cg[d] * (ma * dvy + mb * dvx);
-            df[5] += cg[d] * (ma * dvz + mc * dvx);
-            df[6] += cg2l[d] * mb * dvy + clam[d] * (ma * dvx + mc * dvz);
-            df[7] += cg[d] * (mb * dvz + mc * dvy);
-            df[8] += cg2l[d] * mc * dvz + clam[d] * (ma * dvx + mb * dvy);
+            for (int c = 0; c < 3; c++)
+                df[c] = fmaf(w2, DFl[2][c], fmaf(w1, DFl[1][c], fmaf(w0, DFl[0][c], Acoef * df[c])));
         }
-        // ---- outer-face SATs (faces of the block only)
-        bool defer = false;
-        const bool face = (i == 0) | (i == n0 - 1) | (j == 0) | (j == n1 - 1) | (k == 0) | (k == n2 - 1);
-        if (face) {
-            const int pos[3] = {i, j, k};
+        {
+            // velocity gradient e[a][b] = d v_a / d x_b (times dt)
 #pragma unroll
-            for (int fc = 0; fc < 6; fc++) {
-                const int d = fc / 2;
-                const bool at = (fc % 2 == 0) ? (pos[d] == 0) : (pos[d] == B.n[d] - 1);
-                if (!at) continue;
-                if (B.defer[fc]) defer = true;
-                if (!B.bactive[fc]) continue;
-                const int fa = (d == 0) ? j : i;
-                const int fb = (d == 2) ? j : k;
-                // the SAT reads and writes through pointers: work on copies so that
-                // f and df stay in registers on every other node
-                float fl[9], dl[9];
+            for (int d = 0; d < 3; d++)
 #pragma unroll
-                for (int c = 0; c < 9; c++) {
-                    fl[c] = f[c];
-                    dl[c] = df[c];
-                }
-                boundary_sat<float, 3, 2>(B, fc, fa, fb, (float)sa.dt, fl, dl, false);
+                for (int c = 0; c < 3; c++) Dv[d][c] *= sd[d];
+            float e[3][3];
 #pragma unroll
-                for (int c = 0; c < 9; c++) df[c] = dl[c];
-            }
+            for (int va = 0; va < 3; va++)
+#pragma unroll
+                for (int b = 0; b < 3; b++) e[va][b] = fmaf(m[6 + b], Dv[2][va], fmaf(m[3 + b], Dv[1][va], m[b] * Dv[0][va]));
+            const float lt = lamc * (e[0][0] + e[1][1] + e[2][2]);
+            df[3] = fmaf(Acoef, df[3], fmaf(g2c, e[0][0], lt));
+            df[4] = fmaf(Acoef, df[4], gc * (e[0][1] + e[1][0]));
+            df[5] = fmaf(Acoef, df[5], gc * (e[0][2] + e[2][0]));
+            df[6] = fmaf(Acoef, df[6], fmaf(g2c, e[1][1], lt));
+            df[7] = fmaf(Acoef, df[7], gc * (e[1][2] + e[2][1]));
+            df[8] = fmaf(Acoef, df[8], fmaf(g2c, e[2][2], lt));
         }
         if (owner) {
             const int id = colbase + i * s0;
 #pragma unroll
             for (int c = 0; c < 9; c++) DFg[c * cs + id] = df[c];
-            if (!defer) {
+            // face nodes: k_faces3d adds the outer SATs and finishes them
+            if (!(face | (i == 0) | (i == n0 - 1))) {
                 float fn[9];
 #pragma unroll
                 for (int c = 0; c < 9; c++) fn[c] = fmaf(Bcoef, df[c], f[c]);
-                if (sa.last && sa.plastic) {   // return map: indexes its copy by the layout
+                if (PLASTIC && sa.last) {   // return map: indexes its copy by the layout
                     float fl[9];
 #pragma unroll
                     for (int c = 0; c < 9; c++) fl[c] = fn[c];
@@ -425,13 +442,81 @@ __global__ void __launch_bounds__(NT, MINB) k_fast3d(VolumeArgs<float> a, BlockD
     }
 }
 
-template <int ORDER, int MINB>
+// Face nodes of a 3D block, after k_fast3d wrote their rate without the
+// outer SAT: add the SAT of every face the node lies on, in face order
+// (block::set_boundaries), write the rate, and unless a face is an interface
+// (whose kernel finishes the node) perform the RK update.  Thread t walks the
+// six face arrays in turn; a node on several faces is handled by the thread
+// of its first face.
+template <bool PLASTIC>
+__global__ void __launch_bounds__(128) k_faces3d(VolumeArgs<float> a, BlockDev B, StageArgs sa, long long nface) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= nface) return;
+    const int n[3] = {B.n[0], B.n[1], B.n[2]};
+    const long long sz[3] = {(long long)n[1] * n[2], (long long)n[0] * n[2], (long long)n[0] * n[1]};
+    long long r = t;
+    int fc = 0;
+    while (fc < 5 && r >= sz[fc / 2]) {
+        r -= sz[fc / 2];
+        fc++;
+    }
+    const int d = fc / 2;
+    const int nb2 = (d == 2) ? n[1] : n[2];
+    const int ua = (int)(r / nb2), ub = (int)(r % nb2);
+    int p[3];
+    p[d] = (fc % 2 == 0) ? 0 : n[d] - 1;
+    if (d == 0) {
+        p[1] = ua;
+        p[2] = ub;
+    } else if (d == 1) {
+        p[0] = ua;
+        p[2] = ub;
+    } else {
+        p[0] = ua;
+        p[1] = ub;
+    }
+    for (int f2 = 0; f2 < fc; f2++) {
+        const int d2 = f2 / 2;
+        if (d2 == d) continue;
+        if (p[d2] == ((f2 % 2 == 0) ? 0 : n[d2] - 1)) return;   // belongs to an earlier face
+    }
+    const Layout& L = a.L;
+    const long long cs = L.cstride;
+    const long long id = node_index(L, B.lo[0] + p[0], B.lo[1] + p[1], B.lo[2] + p[2]);
+    float f[9], df[9];
+#pragma unroll
+    for (int c = 0; c < 9; c++) {
+        f[c] = a.F[c * cs + id];
+        df[c] = a.DF[c * cs + id];
+    }
+    bool defer = false;
+    for (int f2 = 0; f2 < 6; f2++) {
+        const int d2 = f2 / 2;
+        if (p[d2] != ((f2 % 2 == 0) ? 0 : n[d2] - 1)) continue;
+        if (B.defer[f2]) defer = true;
+        if (!B.bactive[f2]) continue;
+        const int fa = (d2 == 0) ? p[1] : p[0];
+        const int fb = (d2 == 2) ? p[1] : p[2];
+        boundary_sat<float, 3, 2>(B, f2, fa, fb, (float)sa.dt, f, df, false);
+    }
+#pragma unroll
+    for (int c = 0; c < 9; c++) a.DF[c * cs + id] = df[c];
+    if (defer) return;
+    const float Bcoef = (float)sa.B;
+    float fn[9];
+#pragma unroll
+    for (int c = 0; c < 9; c++) fn[c] = fmaf(Bcoef, df[c], f[c]);
+    if (PLASTIC && sa.last) finish_node<float>(L, B, sa, a.s0, a.S, nullptr, a.FP, a.plastic_tensor, id, fn, false);
+#pragma unroll
+    for (int c = 0; c < 9; c++) a.Fn[c * cs + id] = fn[c];
+}
+
+template <int ORDER, bool PLASTIC>
 void launch_order(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s) {
     using C = FastCfg<ORDER>;
     static bool configured = false;
     if (!configured) {
-        cudaFuncSetAttribute(k_fast3d<ORDER, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)C::SMEM);
+        cudaFuncSetAttribute(k_fast3d<ORDER, PLASTIC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
         configured = true;
     }
     const int tk = (b.n[2] + TK - 1) / TK, tj = (b.n[1] + TJ - 1) / TJ;
@@ -439,14 +524,25 @@ void launch_order(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const int slots = MINB * nsm;
+    const int slots = 2 * nsm;
     int chunks = (4 * slots + tk * tj - 1) / (tk * tj);
     if (chunks < 1) chunks = 1;
     int chunk = (b.n[0] + chunks - 1) / chunks;
     if (chunk < 16) chunk = 16;
     chunks = (b.n[0] + chunk - 1) / chunk;
     dim3 grid(tk, tj, chunks);
-    k_fast3d<ORDER, MINB><<<grid, NT, C::SMEM, s>>>(a, b, sa, chunk);
+    k_fast3d<ORDER, PLASTIC><<<grid, NT, C::SMEM, s>>>(a, b, sa, chunk);
+    const long long nface = 2LL * ((long long)b.n[1] * b.n[2] + (long long)b.n[0] * b.n[2] + (long long)b.n[0] * b.n[1]);
+    k_faces3d<PLASTIC><<<(unsigned)((nface + 127) / 128), 128, 0, s>>>(a, b, sa, nface);
+}
+
+template <bool PLASTIC>
+void launch_plastic(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s) {
+    switch (a.order) {
+        case 2: launch_order<2, PLASTIC>(a, b, sa, s); break;
+        case 3: launch_order<3, PLASTIC>(a, b, sa, s); break;
+        default: launch_order<4, PLASTIC>(a, b, sa, s); break;
+    }
 }
 
 }  // namespace
@@ -465,11 +561,10 @@ void launch_volume_fast3d(const VolumeArgs<float>& a, const BlockDev& b, const S
         launch_volume_exact<float>(a, b, sa, s);   // artificial dissipation: exact-order kernel
         return;
     }
-    switch (a.order) {
-        case 2: launch_order<2, 2>(a, b, sa, s); break;
-        case 3: launch_order<3, 2>(a, b, sa, s); break;
-        default: launch_order<4, 2>(a, b, sa, s); break;
-    }
+    if (sa.plastic)
+        launch_plastic<true>(a, b, sa, s);
+    else
+        launch_plastic<false>(a, b, sa, s);
 }
 
 }  // namespace fdf
