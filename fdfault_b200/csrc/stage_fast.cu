@@ -445,58 +445,53 @@ __global__ void __launch_bounds__(NT, 2) k_fast3d(VolumeArgs<float> a, BlockDev 
 // Face nodes of a 3D block, after k_fast3d wrote their rate without the
 // outer SAT: add the SAT of every face the node lies on, in face order
 // (block::set_boundaries), write the rate, and unless a face is an interface
-// (whose kernel finishes the node) perform the RK update.  Thread t walks the
-// six face arrays in turn; a node on several faces is handled by the thread
-// of its first face.
+// (whose kernel finishes the node) perform the RK update.  blockIdx.z is the
+// face; threadIdx.x runs along the face's k extent (its j extent on the two
+// k faces), threadIdx.y along the other.  A node on several faces is handled
+// by its first face.
 template <bool PLASTIC>
-__global__ void __launch_bounds__(128) k_faces3d(VolumeArgs<float> a, BlockDev B, StageArgs sa, long long nface) {
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= nface) return;
-    const int n[3] = {B.n[0], B.n[1], B.n[2]};
-    const long long sz[3] = {(long long)n[1] * n[2], (long long)n[0] * n[2], (long long)n[0] * n[1]};
-    long long r = t;
-    int fc = 0;
-    while (fc < 5 && r >= sz[fc / 2]) {
-        r -= sz[fc / 2];
-        fc++;
-    }
-    const int d = fc / 2;
-    const int nb2 = (d == 2) ? n[1] : n[2];
-    const int ua = (int)(r / nb2), ub = (int)(r % nb2);
-    int p[3];
-    p[d] = (fc % 2 == 0) ? 0 : n[d] - 1;
+__global__ void __launch_bounds__(128) k_faces3d(VolumeArgs<float> a, BlockDev B, StageArgs sa) {
+    const int fc = blockIdx.z, d = fc >> 1;
+    const int n0 = B.n[0], n1 = B.n[1], n2 = B.n[2];
+    const int nb = (d == 2) ? n1 : n2;
+    const int na = (d == 0) ? n1 : n0;
+    const int ub = blockIdx.x * 32 + threadIdx.x, ua = blockIdx.y * 4 + threadIdx.y;
+    if (ub >= nb || ua >= na) return;
+    const int at = (fc & 1) ? ((d == 0) ? n0 : ((d == 1) ? n1 : n2)) - 1 : 0;
+    int i, j, k;
     if (d == 0) {
-        p[1] = ua;
-        p[2] = ub;
+        i = at;
+        j = ua;
+        k = ub;
     } else if (d == 1) {
-        p[0] = ua;
-        p[2] = ub;
+        i = ua;
+        j = at;
+        k = ub;
     } else {
-        p[0] = ua;
-        p[1] = ub;
+        i = ua;
+        j = ub;
+        k = at;
     }
-    for (int f2 = 0; f2 < fc; f2++) {
-        const int d2 = f2 / 2;
-        if (d2 == d) continue;
-        if (p[d2] == ((f2 % 2 == 0) ? 0 : n[d2] - 1)) return;   // belongs to an earlier face
-    }
+    if (d >= 1 && (i == 0 || i == n0 - 1)) return;   // belongs to an x face
+    if (d == 2 && (j == 0 || j == n1 - 1)) return;   // belongs to a y face
     const Layout& L = a.L;
     const long long cs = L.cstride;
-    const long long id = node_index(L, B.lo[0] + p[0], B.lo[1] + p[1], B.lo[2] + p[2]);
+    const long long id = node_index(L, B.lo[0] + i, B.lo[1] + j, B.lo[2] + k);
     float f[9], df[9];
 #pragma unroll
     for (int c = 0; c < 9; c++) {
         f[c] = a.F[c * cs + id];
         df[c] = a.DF[c * cs + id];
     }
+    const bool on[6] = {i == 0, i == n0 - 1, j == 0, j == n1 - 1, k == 0, k == n2 - 1};
     bool defer = false;
+#pragma unroll
     for (int f2 = 0; f2 < 6; f2++) {
-        const int d2 = f2 / 2;
-        if (p[d2] != ((f2 % 2 == 0) ? 0 : n[d2] - 1)) continue;
+        if (!on[f2]) continue;
         if (B.defer[f2]) defer = true;
         if (!B.bactive[f2]) continue;
-        const int fa = (d2 == 0) ? p[1] : p[0];
-        const int fb = (d2 == 2) ? p[1] : p[2];
+        const int fa = (f2 < 2) ? j : i;
+        const int fb = (f2 >= 4) ? j : k;
         boundary_sat<float, 3, 2>(B, f2, fa, fb, (float)sa.dt, f, df, false);
     }
 #pragma unroll
@@ -532,8 +527,8 @@ void launch_order(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs
     chunks = (b.n[0] + chunk - 1) / chunk;
     dim3 grid(tk, tj, chunks);
     k_fast3d<ORDER, PLASTIC><<<grid, NT, C::SMEM, s>>>(a, b, sa, chunk);
-    const long long nface = 2LL * ((long long)b.n[1] * b.n[2] + (long long)b.n[0] * b.n[2] + (long long)b.n[0] * b.n[1]);
-    k_faces3d<PLASTIC><<<(unsigned)((nface + 127) / 128), 128, 0, s>>>(a, b, sa, nface);
+    const int nbmax = b.n[2] > b.n[1] ? b.n[2] : b.n[1], namax = b.n[0] > b.n[1] ? b.n[0] : b.n[1];
+    k_faces3d<PLASTIC><<<dim3((nbmax + 31) / 32, (namax + 3) / 4, 6), dim3(32, 4), 0, s>>>(a, b, sa);
 }
 
 template <bool PLASTIC>

@@ -45,11 +45,12 @@ CASES = {
     "planar_o3_rk4": lambda t: planar(t, "planar_o3_rk4", sbporder=3, rkorder=4, nt=12),
     "planar_o2": lambda t: planar(t, "planar_o2", sbporder=2),
     "xfault": lambda t: xfault(t, "xfault"),
-    # two tiles in j whose last tile overlaps the first (closure rows in both)
-    "small_o4": lambda t: planar(t, "small_o4", nx=25, ny=13, nz=37, nt=12),
-    "small_o3": lambda t: planar(t, "small_o3", nx=25, ny=13, nz=37, nt=12, sbporder=3),
+    # three tiles in j and two in k whose last tile overlaps the one before
+    # (closure rows in both)
+    "small_o4": lambda t: planar(t, "small_o4", nx=25, ny=25, nz=37, nt=12),
+    "small_o3": lambda t: planar(t, "small_o3", nx=25, ny=25, nz=37, nt=12, sbporder=3),
     # curvilinear rough fault from surface files, plasticity, depth-dependent stress file
-    "rough_plastic": lambda t: P.rough3d(nx=25, ny=13, nz=37, h=0.25, nt=10, name="rough_plastic",
+    "rough_plastic": lambda t: P.rough3d(nx=25, ny=25, nz=37, h=0.25, nt=10, name="rough_plastic",
                                          datadir=t + "/", workdir=t, nuc_half=0.75),
 }
 
