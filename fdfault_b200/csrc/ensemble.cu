@@ -2,9 +2,14 @@
 // per-node code is the exact-order volume and interface code, so a member's
 // result is bit-identical to the same member run alone in FP32).
 //
-// One stage of every member is two launches: a volume kernel whose CTAs walk
-// the work list of volume tiles of all active members (grid-stride, one wave
-// of CTAs), then an interface kernel over all fault tiles.  A one-thread
+// One stage of every member is a volume launch per kind of member, then an
+// interface launch over all fault tiles.  Members whose 2D blocks all fit the
+// tiled 2D kernel (stage_fast2d.cu) are stepped by its batched form, whose
+// warps walk a list of (member, block, 32-column tile, row chunk) items --
+// bit-identical to the member run alone with that kernel; every other member
+// (3D, plastic, small blocks) by the one-thread-per-node kernel below, whose
+// CTAs walk the work list of node tiles (grid-stride, one wave of CTAs) --
+// bit-identical to the member run alone with the reference-order kernel.  A one-thread
 // kernel advances the members' step counters and field-buffer parities at the
 // end of each step, so the step sequence holds no host-side state and a chunk
 // of steps is captured once in a CUDA graph and replayed.
@@ -28,10 +33,7 @@ void ck(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
 }
 
-struct RK {
-    double A[5], B[5], C[6];
-    int nstages;
-};
+using RK = EnsRK;
 
 // the per-stage scalars of one member, as the single-problem solver forms them
 __device__ __forceinline__ StageArgs member_stage(const EnsMember& M, const RK& rk, int st) {
@@ -178,17 +180,48 @@ Ensemble::~Ensemble() {
     if (dmem_) cudaFree(dmem_);
     if (dvt_) cudaFree(dvt_);
     if (dit_) cudaFree(dit_);
+    for (auto& g : g2d_) cudaFree(g.items);
     if (stream_) cudaStreamDestroy(stream_);
+}
+
+bool Ensemble::member_tiled2d(int m) const {
+    const Solver& s = *members_[m];
+    if (s.L_.ndim != 2 || s.P_.cdiss > 0. || s.P_.plastic()) return false;
+    for (const auto& B : s.blocks_)
+        if (!fast2d_supported(s.L_, B, s.P_.sbporder)) return false;
+    return true;
 }
 
 void Ensemble::build_tiles() {
     std::vector<EnsTile> vt, it;
+    std::vector<std::vector<Ens2dItem>> items2d;
+    std::vector<std::pair<int, int>> keys2d;   // (order, mode) of each 2D group
+    // rows per tiled-2D work item: `tile` nodes over 32 columns
+    const int rows = (int)std::max<long long>(16, cfg_.tile / 32);
     for (size_t m = 0; m < members_.size(); m++) {
         const Solver& s = *members_[m];
-        for (size_t b = 0; b < s.blocks_.size(); b++) {
-            const BlockDev& B = s.blocks_[b];
-            const long long nn = (long long)B.n[0] * B.n[1] * B.n[2];
-            for (long long a = 0; a < nn; a += cfg_.tile) vt.push_back({(int)m, 0, (int)b, a, std::min(nn, a + cfg_.tile)});
+        if (member_tiled2d((int)m)) {
+            const std::pair<int, int> key(s.P_.sbporder, s.L_.mode);
+            size_t g = 0;
+            while (g < keys2d.size() && keys2d[g] != key) g++;
+            if (g == keys2d.size()) {
+                keys2d.push_back(key);
+                items2d.emplace_back();
+            }
+            for (size_t b = 0; b < s.blocks_.size(); b++) {
+                const BlockDev& B = s.blocks_[b];
+                const int ntj = (B.n[1] + 31) / 32;
+                for (int ib = 0; ib < B.n[0]; ib += rows)
+                    for (int jt = 0; jt < ntj; jt++)
+                        items2d[g].push_back({(int)m, (int)b, jt, ib, std::min(B.n[0], ib + rows)});
+            }
+        } else {
+            for (size_t b = 0; b < s.blocks_.size(); b++) {
+                const BlockDev& B = s.blocks_[b];
+                const long long nn = (long long)B.n[0] * B.n[1] * B.n[2];
+                for (long long a = 0; a < nn; a += cfg_.tile)
+                    vt.push_back({(int)m, 0, (int)b, a, std::min(nn, a + cfg_.tile)});
+            }
         }
         for (size_t i = 0; i < s.ifaces_.size(); i++) {
             const long long nn = (long long)s.ifaces_[i].n0 * s.ifaces_[i].n1;
@@ -199,6 +232,16 @@ void Ensemble::build_tiles() {
     if (dvt_) cudaFree(dvt_);
     if (dit_) cudaFree(dit_);
     dvt_ = dit_ = nullptr;
+    for (auto& g : g2d_) cudaFree(g.items);
+    g2d_.clear();
+    for (size_t g = 0; g < keys2d.size(); g++) {
+        Group2d G{keys2d[g].first, keys2d[g].second, 0, (int)items2d[g].size(), nullptr};
+        G.grid = fast2d_ensemble_grid(G.order, G.mode, device_);
+        ck(cudaMalloc(&G.items, items2d[g].size() * sizeof(Ens2dItem)), "cudaMalloc tiles");
+        g2d_.push_back(G);   // owned from here on, freed on rebuild or destruction
+        ck(cudaMemcpy(G.items, items2d[g].data(), items2d[g].size() * sizeof(Ens2dItem), cudaMemcpyHostToDevice),
+           "tiles");
+    }
     nvt_ = (int)vt.size();
     nit_ = (int)it.size();
     ck(cudaMalloc(&dvt_, std::max<size_t>(1, vt.size()) * sizeof(EnsTile)), "cudaMalloc tiles");
@@ -235,7 +278,10 @@ void Ensemble::launch(int nsteps) {
     const int gv = std::min(grid_, std::max(nvt_, 1)), gi = std::min(grid_, std::max(nit_, 1));
     for (int n = 0; n < nsteps; n++) {
         for (int st = 0; st < nstages_; st++) {
-            k_ens_volume<<<gv, cfg_.threads, 0, stream_>>>(dmem_, dvt_, nvt_, rk, st);
+            if (nvt_) k_ens_volume<<<gv, cfg_.threads, 0, stream_>>>(dmem_, dvt_, nvt_, rk, st);
+            for (const auto& g : g2d_)
+                fast2d_ensemble_launch(g.order, g.mode, std::min(g.grid, (g.n + 3) / 4), dmem_, g.items, g.n, rk,
+                                       st, stream_);
             if (nit_) k_ens_iface<<<gi, cfg_.threads, 0, stream_>>>(dmem_, dit_, nit_, rk, st);
         }
         k_ens_advance<<<1, 256, 0, stream_>>>(dmem_, (int)members_.size(), nstages_);

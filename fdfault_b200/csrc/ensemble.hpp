@@ -1,17 +1,19 @@
 #pragma once
 // Batched ensemble of independent FP32 problems (2D or 3D, elastic) advanced
-// together by one persistent cooperative kernel launch per chunk of steps.
+// together, stage by stage, by a few launches per stage.
 //
 // Every member is an ordinary Solver (its own fields, geometry, fault arrays,
-// status word).  The kernel walks all members in lockstep, stage by stage:
-// a grid-stride loop over volume tiles of every active member, a grid-wide
-// barrier, a loop over fault tiles, a barrier.  The per-node work is the
-// same device code as the per-block kernels (volume_node, interface_node),
-// so each member's result is bit-identical to running it alone.  Member step
-// counters and field-buffer parities live on the device and are advanced by
-// the kernel itself, so the launch can be captured once in a CUDA graph and
-// replayed.  Tile size and CTA size come from an autotuner that times each
-// candidate on real steps (the tiling does not change any result).
+// status word).  Per stage: volume launches whose CTAs (or warps) walk work
+// lists covering every active member -- 2D members that fit the tiled 2D
+// kernel through its batched form (stage_fast2d.cu), the others through the
+// one-thread-per-node kernel -- then one launch over all fault tiles.  The
+// per-node work is the same device code as the per-block kernels, so each
+// member's result is bit-identical to running it alone with the matching
+// kernel.  Member step counters and field-buffer parities live on the device
+// and are advanced by a one-thread kernel, so a chunk of steps is captured
+// once in a CUDA graph and replayed.  Work-item size and CTA size come from
+// an autotuner that times each candidate on real steps (the tiling does not
+// change any result).
 #include <cuda_runtime.h>
 
 #include <memory>
@@ -49,6 +51,23 @@ struct EnsTile {
     long long begin, end;
 };
 
+// a work item of the tiled 2D volume kernel: 32-column tile jt of block
+// `part` of member `m`, rows [ib, ie)
+struct Ens2dItem {
+    int m, part, jt, ib, ie;
+};
+
+// Runge-Kutta coefficients shared by all members
+struct EnsRK {
+    double A[5], B[5], C[6];
+    int nstages;
+};
+
+// tiled 2D volume stage over a work list (stage_fast2d.cu)
+int fast2d_ensemble_grid(int order, int mode, int device);
+void fast2d_ensemble_launch(int order, int mode, int grid, const EnsMember* mem, const Ens2dItem* items,
+                            int nitems, const EnsRK& rk, int st, cudaStream_t s);
+
 struct EnsConfig {
     int threads = 256;        // CTA size
     long long tile = 4096;    // nodes per tile
@@ -82,6 +101,12 @@ class Ensemble {
     EnsTile* dvt_ = nullptr;
     EnsTile* dit_ = nullptr;
     int nvt_ = 0, nit_ = 0;
+    // tiled 2D work lists, one per (order, mode) group of members
+    struct Group2d {
+        int order, mode, grid, n;
+        Ens2dItem* items;
+    };
+    std::vector<Group2d> g2d_;
     int nstages_ = 0;
     double A_[5] = {0}, B_[5] = {0}, C_[6] = {0};
     bool graph_on_ = true;
@@ -90,6 +115,7 @@ class Ensemble {
     int grid_ = 0;
     std::vector<int> host_step_, host_cur_, host_nt_;
     void build_tiles();
+    bool member_tiled2d(int m) const;   // stepped by the tiled 2D kernel
     void launch(int nsteps);
     void sync_members_from_device();
 };

@@ -52,6 +52,11 @@ void launch_volume_exact(const VolumeArgs<T>& a, const BlockDev& b, const StageA
 // optimised FP32 3D kernel (2.5D tiles marching along x, shared-memory halos)
 void launch_volume_fast3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s);
 bool fast3d_supported(const Layout& L, const BlockDev& b, int order);
+
+// optimised FP32 2D kernel (mode II / mode III elastic; one warp per 32-column
+// tile marching along x); plastic or dissipative stages go to the exact kernel
+void launch_volume_fast2d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s);
+bool fast2d_supported(const Layout& L, const BlockDev& b, int order);
 // staged FP32 3D kernel (planes brought into shared memory by TMA tensor copies)
 struct StagedMapsHost;
 StagedMapsHost* make_staged_maps(const Layout& L, const float* F0, const float* F1, const float* M, const float* J,

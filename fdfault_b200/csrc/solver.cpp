@@ -763,7 +763,13 @@ void Solver::profile_read(int kernel, double* total_ms, long long* launches) {
 }
 
 int Solver::volume_kernel_active() const {
-    if (vkernel_ == 0 || precision_ != 1 || L_.ndim != 3) return 0;
+    if (vkernel_ == 0 || precision_ != 1) return 0;
+    if (L_.ndim == 2) {   // tiled 2D kernel (elastic, no dissipation) or none
+        if (vkernel_ != 1 || P_.plastic() || P_.cdiss > 0.) return 0;
+        for (auto& B : blocks_)
+            if (!fast2d_supported(L_, B, P_.sbporder)) return 0;
+        return 1;
+    }
     for (auto& B : blocks_) {
         if (vkernel_ == 1 && !fast3d_supported(L_, B, P_.sbporder)) return 0;
         if (vkernel_ == 2 && !staged3d_supported(L_, B, P_.sbporder)) return 0;
@@ -820,8 +826,10 @@ void Solver::stage_impl(double dt, int stage, double t, bool for_step) {
                                                     (const float*)J_, P_.sbporder);
                 launch_volume_staged3d(va, blocks_[b], sa, status_, staged_maps_, stream_);
             }
-            else if (vk == 1)
+            else if (vk == 1 && L_.ndim == 3)
                 launch_volume_fast3d(va, blocks_[b], sa, stream_);
+            else if (vk == 1)
+                launch_volume_fast2d(va, blocks_[b], sa, stream_);
             else
                 launch_volume_exact<T>(va, blocks_[b], sa, stream_);
         } else {

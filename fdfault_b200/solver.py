@@ -271,7 +271,8 @@ class Problem:
         self._check(self._L.fdf_use_graphs(self._h, int(on)))
 
     def set_volume_kernel(self, kind: int) -> int:
-        """FP32 3D volume kernel: 0 reference order, 1 tiled, 2 staged; returns the kind that runs."""
+        """FP32 volume kernel: 0 reference order, 1 tiled (3D, or 2D elastic), 2 staged (3D);
+        returns the kind that runs."""
         act = ctypes.c_int()
         self._check(self._L.fdf_set_volume_kernel(self._h, kind, ctypes.byref(act)))
         return act.value

@@ -1,8 +1,10 @@
 """Batched ensemble: every member, advanced together with the others by the
 batched launches (CUDA-graph chunks and direct remainders, any tile
 configuration the autotuner may pick), is bit-identical to the same problem
-run alone in FP32 with the one-thread-per-node volume kernel -- for members of
-different sizes, a 3D member, and a member that reaches its last step early."""
+run alone in FP32 with the matching volume kernel -- the tiled 2D kernel for
+2D members whose blocks fit it, the one-thread-per-node kernel for the rest --
+for members of different sizes (some too narrow for the tiled kernel), a 3D
+member, and a member that reaches its last step early."""
 
 import os
 
@@ -27,7 +29,7 @@ def members(tmp):
 
 def alone(infile, nsteps):
     with fs.Problem(infile, precision=fs.FP32) as p:
-        p.use_fast_kernel(False)
+        p.set_volume_kernel(1 if p.ndim == 2 else 0)
         p.step(min(nsteps, p.nt))
         p.synchronize()
         return state(p)
