@@ -49,6 +49,16 @@ struct VolumeArgs {
 template <typename T>
 void launch_volume_exact(const VolumeArgs<T>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s);
 
+// the exact-order kernel over all nb <= FDF_ALLB_MAX blocks in one launch;
+// blks_dev is a device copy of the host table blks
+constexpr int FDF_ALLB_MAX = 8;
+struct BlockRanges {
+    long long start[FDF_ALLB_MAX + 1];   // first node of each block in the launch; start[MAX] = total
+};
+template <typename T>
+void launch_volume_exact_all(const VolumeArgs<T>& a, const BlockDev* blks_dev, const BlockDev* blks, int nb,
+                             const StageArgs& sa, cudaStream_t s);
+
 // optimised FP32 3D kernel (2.5D tiles marching along x, shared-memory halos)
 void launch_volume_fast3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s);
 bool fast3d_supported(const Layout& L, const BlockDev& b, int order);

@@ -236,6 +236,10 @@ Solver::Solver(const std::string& infile, int precision, int device) : precision
     if (P_.front_on && P_.front_field == "V")
         for (auto& I : ifaces_)
             if (I.kind >= 1) launch_front(I, 0., P_.front_value, stream_);
+    blocks_dev_ = static_cast<BlockDev*>(dalloc(blocks_.size() * sizeof(BlockDev)));
+    cuda_check(cudaMemcpyAsync(blocks_dev_, blocks_.data(), blocks_.size() * sizeof(BlockDev), cudaMemcpyHostToDevice,
+                               stream_),
+               "block table");
     cuda_check(cudaStreamSynchronize(stream_), "set-up");
     if (int st = check_status()) throw std::runtime_error("set-up failed with status " + std::to_string(st));
 }
@@ -812,7 +816,22 @@ void Solver::stage_impl(double dt, int stage, double t, bool for_step) {
     va.ABS = (sa.roundtrip && sa.last) ? ABS_ : nullptr;
     va.plastic_tensor = P_.plastic_tensor ? 1 : 0;
     const int vk = volume_kernel_active();
-    for (size_t b = 0; b < blocks_.size(); b++) {
+    // the reference-order kernel takes every block in one launch
+    const bool all_exact = (sizeof(T) == 8 || vk == 0) && (int)blocks_.size() <= FDF_ALLB_MAX;
+    if (all_exact) {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (profile_) {
+            e0 = ev_get();
+            e1 = ev_get();
+            cudaEventRecord(e0, stream_);
+        }
+        launch_volume_exact_all<T>(va, blocks_dev_, blocks_.data(), (int)blocks_.size(), sa, stream_);
+        if (profile_) {
+            cudaEventRecord(e1, stream_);
+            ev_pending_.push_back({0, {e0, e1}});
+        }
+    }
+    for (size_t b = 0; b < blocks_.size() && !all_exact; b++) {
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (profile_) {
             e0 = ev_get();

@@ -148,6 +148,7 @@ class Solver {
     std::vector<void*> owned_;   // face normals, fault arrays, parameter shapes
 
     std::vector<BlockDev> blocks_;
+    BlockDev* blocks_dev_ = nullptr;   // device copy of blocks_ (final after set-up)
     std::vector<IfaceDev> ifaces_;
     MlpState mlp_;
     bool stz_learned_ = false;

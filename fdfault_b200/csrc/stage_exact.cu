@@ -26,6 +26,27 @@ __global__ void __launch_bounds__(128) k_volume_exact(VolumeArgs<T> a, BlockDev 
     volume_node<T, NDIM, MODE>(a, B, sa, blockIdx.x * (long long)blockDim.x + threadIdx.x);
 }
 
+// Every block of a problem in one launch: thread t takes node t - start[b] of
+// the block b whose range holds t, with the same per-node arithmetic as the
+// per-block launch (the block table is read from device memory).  Small
+// problems, whose per-block launches each fill a fraction of one wave, then
+// overlap their blocks.
+template <typename T, int NDIM, int MODE>
+__global__ void __launch_bounds__(128) k_volume_exact_all(VolumeArgs<T> a, const BlockDev* __restrict__ blks,
+                                                          BlockRanges r, StageArgs sa) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= r.start[FDF_ALLB_MAX]) return;
+    int b = 0;
+    long long s = 0;
+#pragma unroll
+    for (int q = 1; q < FDF_ALLB_MAX; q++)
+        if (t >= r.start[q]) {
+            b = q;
+            s = r.start[q];
+        }
+    volume_node<T, NDIM, MODE>(a, blks[b], sa, t - s);
+}
+
 }  // namespace
 
 template <typename T>
@@ -40,6 +61,29 @@ void launch_volume_exact(const VolumeArgs<T>& a, const BlockDev& b, const StageA
         k_volume_exact<T, 2, 3><<<grid, 128, 0, s>>>(a, b, sa);
 }
 
+template <typename T>
+void launch_volume_exact_all(const VolumeArgs<T>& a, const BlockDev* blks_dev, const BlockDev* blks, int nb,
+                             const StageArgs& sa, cudaStream_t s) {
+    BlockRanges r{};
+    long long n = 0;
+    for (int b = 0; b < FDF_ALLB_MAX; b++) {
+        r.start[b] = n;
+        if (b < nb) n += (long long)blks[b].n[0] * blks[b].n[1] * blks[b].n[2];
+    }
+    r.start[FDF_ALLB_MAX] = n;   // ranges of absent blocks are empty and never selected
+    const unsigned grid = (unsigned)((n + 127) / 128);
+    if (a.L.ndim == 3)
+        k_volume_exact_all<T, 3, 2><<<grid, 128, 0, s>>>(a, blks_dev, r, sa);
+    else if (a.L.mode == 2)
+        k_volume_exact_all<T, 2, 2><<<grid, 128, 0, s>>>(a, blks_dev, r, sa);
+    else
+        k_volume_exact_all<T, 2, 3><<<grid, 128, 0, s>>>(a, blks_dev, r, sa);
+}
+
+template void launch_volume_exact_all<double>(const VolumeArgs<double>&, const BlockDev*, const BlockDev*, int,
+                                              const StageArgs&, cudaStream_t);
+template void launch_volume_exact_all<float>(const VolumeArgs<float>&, const BlockDev*, const BlockDev*, int,
+                                             const StageArgs&, cudaStream_t);
 template void launch_volume_exact<double>(const VolumeArgs<double>&, const BlockDev&, const StageArgs&, cudaStream_t);
 template void launch_volume_exact<float>(const VolumeArgs<float>&, const BlockDev&, const StageArgs&, cudaStream_t);
 
