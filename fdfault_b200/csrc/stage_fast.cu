@@ -81,7 +81,7 @@ struct HaloNode {
     float s[6], v[3], m[3], J;
 };
 
-template <int ORDER, bool PLASTIC>
+template <int ORDER>
 __global__ void __launch_bounds__(NT, 2) k_fast3d(VolumeArgs<float> a, BlockDev B, StageArgs sa, int chunk) {
     using C = FastCfg<ORDER>;
     constexpr int H = C::H, R = C::R, NB = C::NB, NTB = C::NTB, VH = C::VH, VW = C::VW;
@@ -419,19 +419,8 @@ __global__ void __launch_bounds__(NT, 2) k_fast3d(VolumeArgs<float> a, BlockDev 
             for (int c = 0; c < 9; c++) DFg[c * cs + id] = df[c];
             // face nodes: k_faces3d adds the outer SATs and finishes them
             if (!(face | (i == 0) | (i == n0 - 1))) {
-                float fn[9];
 #pragma unroll
-                for (int c = 0; c < 9; c++) fn[c] = fmaf(Bcoef, df[c], f[c]);
-                if (PLASTIC && sa.last) {   // return map: indexes its copy by the layout
-                    float fl[9];
-#pragma unroll
-                    for (int c = 0; c < 9; c++) fl[c] = fn[c];
-                    finish_node<float>(L, B, sa, a.s0, a.S, nullptr, a.FP, a.plastic_tensor, id, fl, false);
-#pragma unroll
-                    for (int c = 0; c < 9; c++) fn[c] = fl[c];
-                }
-#pragma unroll
-                for (int c = 0; c < 9; c++) Fn[c * cs + id] = fn[c];
+                for (int c = 0; c < 9; c++) Fn[c * cs + id] = fmaf(Bcoef, df[c], f[c]);
             }
         }
         if (more) {
@@ -506,12 +495,32 @@ __global__ void __launch_bounds__(128) k_faces3d(VolumeArgs<float> a, BlockDev B
     for (int c = 0; c < 9; c++) a.Fn[c * cs + id] = fn[c];
 }
 
+// Drucker-Prager return map (finish_node on the last stage) of the interior
+// nodes of a block, after k_fast3d wrote their updated fields: face nodes were
+// finished by k_faces3d and fault nodes by the interface kernel.  Kept out of
+// the marching kernel, whose register budget the FP64 return map would exceed.
+__global__ void __launch_bounds__(256) k_return_map3(VolumeArgs<float> a, BlockDev B, StageArgs sa) {
+    const int n1i = B.n[1] - 2, n2i = B.n[2] - 2;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)(B.n[0] - 2) * n1i * n2i) return;
+    const int k = 1 + (int)(t % n2i), j = 1 + (int)((t / n2i) % n1i), i = 1 + (int)(t / ((long long)n2i * n1i));
+    const Layout& L = a.L;
+    const long long cs = L.cstride;
+    const long long id = node_index(L, B.lo[0] + i, B.lo[1] + j, B.lo[2] + k);
+    float fn[9];
+#pragma unroll
+    for (int c = 0; c < 9; c++) fn[c] = a.Fn[c * cs + id];
+    finish_node<float>(L, B, sa, a.s0, a.S, nullptr, a.FP, a.plastic_tensor, id, fn, false);
+#pragma unroll
+    for (int c = 3; c < 9; c++) a.Fn[c * cs + id] = fn[c];
+}
+
 template <int ORDER, bool PLASTIC>
 void launch_order(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s) {
     using C = FastCfg<ORDER>;
     static bool configured = false;
     if (!configured) {
-        cudaFuncSetAttribute(k_fast3d<ORDER, PLASTIC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+        cudaFuncSetAttribute(k_fast3d<ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
         configured = true;
     }
     const int tk = (b.n[2] + TK - 1) / TK, tj = (b.n[1] + TJ - 1) / TJ;
@@ -526,9 +535,13 @@ void launch_order(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs
     if (chunk < 16) chunk = 16;
     chunks = (b.n[0] + chunk - 1) / chunk;
     dim3 grid(tk, tj, chunks);
-    k_fast3d<ORDER, PLASTIC><<<grid, NT, C::SMEM, s>>>(a, b, sa, chunk);
+    k_fast3d<ORDER><<<grid, NT, C::SMEM, s>>>(a, b, sa, chunk);
     const int nbmax = b.n[2] > b.n[1] ? b.n[2] : b.n[1], namax = b.n[0] > b.n[1] ? b.n[0] : b.n[1];
     k_faces3d<PLASTIC><<<dim3((nbmax + 31) / 32, (namax + 3) / 4, 6), dim3(32, 4), 0, s>>>(a, b, sa);
+    if (PLASTIC && sa.last) {
+        const long long nin = (long long)(b.n[0] - 2) * (b.n[1] - 2) * (b.n[2] - 2);
+        k_return_map3<<<(unsigned)((nin + 255) / 256), 256, 0, s>>>(a, b, sa);
+    }
 }
 
 template <bool PLASTIC>
