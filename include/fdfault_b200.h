@@ -144,10 +144,12 @@ int fdf_use_graphs(fdf_handle* h, int on);
  * will run. */
 int fdf_use_fast_kernel(fdf_handle* h, int on, int* active);
 
-/* FP32 3D volume kernel by kind: 0 one thread per node (reference operation
- * order), 1 tiled with per-thread global loads (the default), 2 staged (planes
+/* FP32 volume kernel by kind: 0 one thread per node (reference operation
+ * order), 1 tiled (the default: 3D blocks of at least 8 x 32 in y x z, and 2D
+ * elastic blocks at least 32 nodes wide in y), 2 staged (3D only: planes
  * brought into shared memory by TMA tensor copies).  active = the kind that
- * will run (0 where the chosen one does not apply to the problem). */
+ * will run (0 where the chosen one does not apply to the problem; FP64
+ * problems always run kind 0). */
 int fdf_set_volume_kernel(fdf_handle* h, int kind, int* active);
 
 /* Algorithmic bytes moved per node per stage by the volume kernel. */
