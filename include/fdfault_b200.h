@@ -199,12 +199,15 @@ int fdf_mlp_train(fdf_handle* h, int epochs, int batch, float lr, unsigned long 
  *
  * All members run in FP32 (fields) with FP64 friction, share the Runge-Kutta
  * order, are elastic and use locked, frictionless or slip-weakening
- * interfaces.  Each stage of all members is one batched volume launch and
- * one batched interface launch over a work list of tiles; step counters and
- * field-buffer parities live on the device, and chunks of 16 steps replay
- * one captured CUDA graph.  A member's results are bit-identical to running
- * it alone in FP32 with the one-thread-per-node volume kernel.  Members step
- * min(nsteps, nt - step) steps. */
+ * interfaces.  Each stage of all members is a few batched volume launches
+ * (2D members whose blocks are at least 32 nodes wide in y: the tiled 2D
+ * kernel, one launch per SBP order and mode present; all others: the
+ * one-thread-per-node kernel) and one batched interface launch, each over a
+ * work list; step counters and field-buffer parities live on the device, and
+ * chunks of 16 steps replay one captured CUDA graph.  A member's results are
+ * bit-identical to running it alone in FP32 with the same volume kernel
+ * (fdf_set_volume_kernel 1 for the first kind, 0 for the second).  Members
+ * step min(nsteps, nt - step) steps. */
 typedef struct fdf_ensemble fdf_ensemble;
 int fdf_ensemble_create(const char* const* infiles, int n, int device, fdf_ensemble** out);
 void fdf_ensemble_destroy(fdf_ensemble* e);
@@ -216,7 +219,8 @@ int fdf_ensemble_member(fdf_ensemble* e, int member, fdf_handle** out);
 int fdf_ensemble_run(fdf_ensemble* e, int nsteps);
 int fdf_ensemble_time_steps(fdf_ensemble* e, int nsteps, double* ms);
 /* times `steps` real steps with each candidate CTA size and tile size, keeps
- * the fastest (tiling never changes results) */
+ * the fastest (tiling never changes results); `tile` is the node count of a
+ * work item (the tiled 2D kernel takes tile / 32 rows of a 32-column tile) */
 int fdf_ensemble_autotune(fdf_ensemble* e, int steps, int* threads, long long* tile);
 int fdf_ensemble_set_config(fdf_ensemble* e, int threads, long long tile);
 int fdf_ensemble_use_graph(fdf_ensemble* e, int on);
