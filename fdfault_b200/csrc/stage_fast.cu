@@ -32,6 +32,7 @@
 // with FMA contraction; the FP64 exact-order kernel is stage_exact.cu.
 #include <cuda_runtime.h>
 
+#include <atomic>
 
 #include "kernels.hpp"
 #include "sbp_coeffs.cuh"
@@ -518,15 +519,17 @@ __global__ void __launch_bounds__(256) k_return_map3(VolumeArgs<float> a, BlockD
 template <int ORDER, bool PLASTIC>
 void launch_order(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s) {
     using C = FastCfg<ORDER>;
-    static bool configured = false;
-    if (!configured) {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    // the shared-memory opt-in is a per-device function attribute: set it once per device
+    static std::atomic<unsigned> configured{0};
+    const unsigned bit = 1u << (dev & 31);
+    if (!(configured.load() & bit)) {
         cudaFuncSetAttribute(k_fast3d<ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
-        configured = true;
+        configured.fetch_or(bit);
     }
     const int tk = (b.n[2] + TK - 1) / TK, tj = (b.n[1] + TJ - 1) / TJ;
     // split the x march into chunks so the grid fills the GPU a few times over
-    int dev = 0, nsm = 148;
-    cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const int slots = 2 * nsm;
     int chunks = (4 * slots + tk * tj - 1) / (tk * tj);

@@ -24,6 +24,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -509,14 +510,16 @@ template <int ORDER>
 void launch_order(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, int* status,
                   const StagedMapsHost& mh, cudaStream_t s) {
     using C = StCfg<ORDER>;
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(k_tma3d<ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
-        configured = true;
-    }
-    const int tk = (b.n[2] + TK - 1) / TK, tj = (b.n[1] + TJ - 1) / TJ;
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
+    // the shared-memory opt-in is a per-device function attribute: set it once per device
+    static std::atomic<unsigned> configured{0};
+    const unsigned bit = 1u << (dev & 31);
+    if (!(configured.load() & bit)) {
+        cudaFuncSetAttribute(k_tma3d<ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+        configured.fetch_or(bit);
+    }
+    const int tk = (b.n[2] + TK - 1) / TK, tj = (b.n[1] + TJ - 1) / TJ;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     // one resident CTA per SM: enough x chunks for a few waves
     int chunks = (3 * nsm + tk * tj - 1) / (tk * tj);
