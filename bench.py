@@ -36,6 +36,7 @@ WORKLOAD = dict(nx=401, ny=201, nz=201, h=0.1)
 PROFILE_WORKLOAD = dict(nx=201, ny=101, nz=101, h=0.2)
 CPU_SAMPLE = dict(nx=101, ny=51, nz=51, h=0.4)
 PROFILE_TRAFFIC = os.path.join(HERE, "profiles", "volume_fast3d_planar3d.md")
+KERNEL_NAMES = {0: "volume_exact", 1: "volume_tiled3d", 2: "volume_staged3d", 3: "volume_regwindow3d"}
 
 
 def parse():
@@ -54,8 +55,9 @@ def parse():
                          "rupture in FP64; ensemble: 256 2D ruptures of uneven sizes, batched; rough: "
                          "rough fault with plasticity, two blocks of 601x301x301, FP32")
     ap.add_argument("--members", type=int, default=256, help="ensemble members (all ranks together)")
-    ap.add_argument("--volume-kernel", type=int, default=1, choices=[0, 1, 2],
-                    help="FP32 3D volume kernel: 0 reference order, 1 tiled (default), 2 staged (TMA)")
+    ap.add_argument("--volume-kernel", type=int, default=1, choices=[0, 1, 2, 3],
+                    help="FP32 3D volume kernel: 0 reference order, 1 tiled (default), 2 staged (TMA), "
+                         "3 register window (TMA-staged planes)")
     return ap.parse_args()
 
 
@@ -548,7 +550,7 @@ def run_rough(args, local):
            "kernel_ms": {"volume_avg": vol_avg, "volume_launches": vol_n,
                          "interface_avg_per_stage": if_ms / max(if_n, 1)},
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                        "peak_source": peak_kind, "kernel": {0: "volume_exact", 1: "volume_tiled3d", 2: "volume_staged3d"}[vk],
+                        "peak_source": peak_kind, "kernel": KERNEL_NAMES[vk],
                         "algorithmic_bytes_per_node_stage": bps}}
     if not args.no_cpu_baseline:
         import oracle
@@ -674,14 +676,14 @@ def main():
     achieved = bytes_per_launch / (vol_avg_ms * 1e-3) / 1e9
     traffic_pn = profiled_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": peak_kind, "kernel": {0: "volume_exact", 1: "volume_tiled3d", 2: "volume_staged3d"}[vk],
+                "peak_source": peak_kind, "kernel": KERNEL_NAMES[vk],
                 "algorithmic_bytes_per_node_stage": bps,
                 "traffic": (traffic_pn * nodes / nblocks) if traffic_pn else None}
     # per step: per stage the volume launches (tiled 3D: a marching and a face-node
     # kernel per block; staged: one per block; reference order: one for all blocks)
     # and one interface launch per interface, plus the graph's step-counter kernel;
     # one counter reset per call
-    vol_per_stage = {0: 1, 1: 2 * nblocks, 2: nblocks}[vk]
+    vol_per_stage = {0: 1, 1: 2 * nblocks, 2: nblocks, 3: 2 * nblocks}[vk]
     launches = args.steps * (nstages * (vol_per_stage + p.nifaces) + 1) + 1
     out = {"metric": METRIC, "value": value, "unit": "node-stage/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",

@@ -3,6 +3,8 @@
 // status and keeps the message for fdf_last_error().
 #include "../../include/fdfault_b200.h"
 
+#include <cuda_runtime.h>
+
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -25,10 +27,36 @@ namespace {
 
 thread_local std::string g_create_error;
 
+// Makes a handle's device current for the duration of one call and restores
+// the caller's device afterwards, so one host thread may drive handles on
+// several devices: every allocation, launch and per-device lookup of a call
+// then happens on the handle's own device.
+class DeviceGuard {
+  public:
+    explicit DeviceGuard(int device) {
+        if (cudaGetDevice(&prev_) != cudaSuccess) prev_ = -1;
+        if (prev_ != device) {
+            if (cudaSetDevice(device) != cudaSuccess)
+                throw std::runtime_error("CUDA error in cudaSetDevice for the handle's device");
+            changed_ = true;
+        }
+    }
+    ~DeviceGuard() {
+        if (changed_ && prev_ >= 0) cudaSetDevice(prev_);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+
+  private:
+    int prev_ = -1;
+    bool changed_ = false;
+};
+
 template <typename F>
 int guarded(fdf_handle* h, F&& f) {
     if (!h || !h->s) return FDF_ERR_ARG;
     try {
+        DeviceGuard dg(h->s->device());
         f(*h->s);
         return 0;
     } catch (const std::exception& e) {
@@ -43,6 +71,7 @@ template <typename F>
 int eguarded(fdf_ensemble* h, F&& f) {
     if (!h || !h->e) return FDF_ERR_ARG;
     try {
+        DeviceGuard dg(h->e->device());
         f(*h->e);
         return 0;
     } catch (const std::exception& e) {
@@ -64,6 +93,7 @@ int fdf_create(const char* infile, int precision, int device, fdf_handle** out) 
     try {
         fdf_handle* h = new fdf_handle;
         try {
+            DeviceGuard dg(device);   // the caller's current device is restored on return
             h->s = new fdf::Solver(infile, precision, device);
         } catch (...) {
             delete h;
@@ -82,7 +112,10 @@ int fdf_create(const char* infile, int precision, int device, fdf_handle** out) 
 void fdf_destroy(fdf_handle* h) {
     if (!h) return;
     try {
-        if (!h->borrowed) delete h->s;
+        if (!h->borrowed && h->s) {
+            DeviceGuard dg(h->s->device());
+            delete h->s;
+        }
     } catch (...) {
     }
     delete h;
@@ -213,11 +246,15 @@ int fdf_use_graphs(fdf_handle* h, int on) {
 }
 
 int fdf_set_volume_kernel(fdf_handle* h, int kind, int* active) {
-    if (kind < 0 || kind > 2) return FDF_ERR_ARG;
+    if (kind < 0 || kind > 3) return FDF_ERR_ARG;
     return guarded(h, [&](fdf::Solver& s) {
         s.set_volume_kernel(kind);
         if (active) *active = s.volume_kernel_active();
     });
+}
+
+int fdf_set_wait_limit(fdf_handle* h, long long polls) {
+    return guarded(h, [&](fdf::Solver& s) { s.set_wait_limit(polls); });
 }
 
 int fdf_use_fast_kernel(fdf_handle* h, int on, int* active) {
@@ -307,6 +344,7 @@ int fdf_ensemble_create(const char* const* infiles, int n, int device, fdf_ensem
         }
         fdf_ensemble* h = new fdf_ensemble;
         try {
+            DeviceGuard dg(device);   // the caller's current device is restored on return
             h->e = new fdf::Ensemble(files, device);
         } catch (...) {
             delete h;
@@ -325,7 +363,10 @@ int fdf_ensemble_create(const char* const* infiles, int n, int device, fdf_ensem
 void fdf_ensemble_destroy(fdf_ensemble* h) {
     if (!h) return;
     try {
-        delete h->e;
+        if (h->e) {
+            DeviceGuard dg(h->e->device());
+            delete h->e;
+        }
     } catch (...) {
     }
     delete h;

@@ -89,6 +89,7 @@ class Ensemble {
     EnsConfig config() const { return cfg_; }
     void use_graph(bool on) { graph_on_ = on; }
     long long node_stages_per_step() const;   // sum over active members
+    int device() const { return device_; }
     void synchronize();
     void check_status();
 

@@ -106,6 +106,9 @@ struct StageArgs {
     // (t = step*dt + cst*dt, tfront = (step+1)*dt, the host's expressions)
     const int* step_dev;
     double cst;
+    // polls of a bounded mbarrier wait in the TMA-staged kernels before they
+    // give up with FDF_ERR_TIMEOUT (<= 0: the built-in limit)
+    long long wait_limit;
 };
 
 enum Status : int {

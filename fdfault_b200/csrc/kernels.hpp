@@ -75,6 +75,17 @@ void free_staged_maps(StagedMapsHost* h);
 void launch_volume_staged3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, int* status,
                             const StagedMapsHost* maps, cudaStream_t s);
 bool staged3d_supported(const Layout& L, const BlockDev& b, int order);
+// register-window FP32 3D kernel (x window in registers, tile planes staged by TMA)
+struct RegMapsHost;
+RegMapsHost* make_reg_maps(const Layout& L, const float* F0, const float* F1, const float* M, const float* J,
+                           const float* DF);
+void free_reg_maps(RegMapsHost* h);
+void launch_volume_reg3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, int* status,
+                         const RegMapsHost* maps, cudaStream_t s);
+bool reg3d_supported(const Layout& L, const BlockDev& b, int order);
+// outer SATs and RK update of the face nodes of a 3D block (elastic), after a
+// marching kernel wrote their rate without the SAT
+void launch_faces3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s);
 
 // interface kernels
 template <typename T>

@@ -135,6 +135,10 @@ Solver::Solver(const std::string& infile, int precision, int device) : precision
     if (precision != 0 && precision != 1) throw std::runtime_error("precision must be 0 (FP64) or 1 (FP32)");
     P_ = read_problem(infile);
     cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    // reserve the allocation-free read-back buffer on this device now (the
+    // lookup loads its module, which lazy module loading would otherwise
+    // defer to the first fdf_get_field_noalloc call)
+    noalloc_field_buffer(device);
     cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
     // RK coefficients: src/rk.cpp:8-98
     switch (P_.rkorder) {
@@ -254,6 +258,7 @@ Solver::~Solver() {
     for (auto g : graph_exec_)
         if (g) cudaGraphExecDestroy(g);
     free_staged_maps(staged_maps_);
+    free_reg_maps(reg_maps_);
     if (step_dev_) cudaFree(step_dev_);
     mlp_free(mlp_);
     if (stz_counts_) cudaFree(stz_counts_);
@@ -777,6 +782,7 @@ int Solver::volume_kernel_active() const {
     for (auto& B : blocks_) {
         if (vkernel_ == 1 && !fast3d_supported(L_, B, P_.sbporder)) return 0;
         if (vkernel_ == 2 && !staged3d_supported(L_, B, P_.sbporder)) return 0;
+        if (vkernel_ == 3 && !reg3d_supported(L_, B, P_.sbporder)) return 0;
     }
     return vkernel_;
 }
@@ -799,6 +805,7 @@ void Solver::stage_impl(double dt, int stage, double t, bool for_step) {
     sa.tfront = (double)(step_index_ + 1) * dt;
     sa.step_dev = capturing_ ? step_dev_ : nullptr;
     sa.cst = C_[stage];
+    sa.wait_limit = wait_limit_;
     T* Fo = (T*)F_[cur_];
     T* Fn = (T*)F_[1 - cur_];
     VolumeArgs<T> va{};
@@ -844,6 +851,11 @@ void Solver::stage_impl(double dt, int stage, double t, bool for_step) {
                     staged_maps_ = make_staged_maps(L_, (const float*)F_[0], (const float*)F_[1], (const float*)M_,
                                                     (const float*)J_, P_.sbporder);
                 launch_volume_staged3d(va, blocks_[b], sa, status_, staged_maps_, stream_);
+            } else if (vk == 3) {
+                if (!reg_maps_)
+                    reg_maps_ = make_reg_maps(L_, (const float*)F_[0], (const float*)F_[1], (const float*)M_,
+                                              (const float*)J_, (const float*)DF_);
+                launch_volume_reg3d(va, blocks_[b], sa, status_, reg_maps_, stream_);
             }
             else if (vk == 1 && L_.ndim == 3)
                 launch_volume_fast3d(va, blocks_[b], sa, stream_);
@@ -923,6 +935,23 @@ void Solver::step_graph(int npairs) {
         const int cur0 = cur_, idx0 = step_index_;
         cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed), "begin capture");
         capturing_ = true;
+        // if a stage throws while the stream captures, end the capture, drop the
+        // partial graph and put the handle's state back before the error leaves
+        struct CaptureGuard {
+            Solver& s;
+            int cur0, idx0;
+            bool armed = true;
+            ~CaptureGuard() {
+                if (!armed) return;
+                cudaGraph_t partial = nullptr;
+                cudaStreamEndCapture(s.stream_, &partial);
+                if (partial) cudaGraphDestroy(partial);
+                cudaGetLastError();
+                s.capturing_ = false;
+                s.cur_ = cur0;
+                s.step_index_ = idx0;
+            }
+        } guard{*this, cur0, idx0};
         for (int n = 0; n < 2; n++) {
             for (int st = 0; st < nstages_; st++) {
                 if (precision_ == 0)
@@ -932,6 +961,7 @@ void Solver::step_graph(int npairs) {
             }
             launch_step_advance(step_dev_, stream_);
         }
+        guard.armed = false;
         capturing_ = false;
         cudaGraph_t g = nullptr;
         cuda_check(cudaStreamEndCapture(stream_, &g), "end capture");

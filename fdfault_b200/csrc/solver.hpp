@@ -73,12 +73,18 @@ class Solver {
     void profile_read(int kernel, double* total_ms, long long* launches);
     void use_fast_kernel(bool on) { set_volume_kernel(on ? 1 : 0); }
     // FP32 3D volume kernel: 0 one thread per node (reference order), 1 tiled
-    // (per-thread global loads), 2 staged (bulk copies into shared memory)
+    // (per-thread global loads), 2 staged (bulk copies into shared memory),
+    // 3 register window (x window in registers, tile planes staged by TMA)
     void set_volume_kernel(int kind) {
         vkernel_ = kind;
         graph_dirty_ = true;
     }
     int volume_kernel_active() const;   // the kind that runs (0 when the chosen one does not apply)
+    // polls of a bounded wait for staged data (<= 0: the built-in limit)
+    void set_wait_limit(long long polls) {
+        wait_limit_ = polls > 0 ? polls : (1LL << 22);
+        graph_dirty_ = true;
+    }
     // replay steps from a captured CUDA graph of two steps (default on)
     void use_graphs(bool on) { graphs_ = on; }
     bool graphs() const { return graphs_; }
@@ -87,6 +93,7 @@ class Solver {
     const ProblemSpec& spec() const { return P_; }
     const Layout& layout() const { return L_; }
     int precision() const { return precision_; }
+    int device() const { return device_; }
     double dt() const { return dt_; }
     int nt() const { return nt_; }
     int nstages() const { return nstages_; }
@@ -129,6 +136,8 @@ class Solver {
     int step_index_ = 0;
     int vkernel_ = 1;
     StagedMapsHost* staged_maps_ = nullptr;   // tensor maps of the FP32 arrays (staged kernel)
+    RegMapsHost* reg_maps_ = nullptr;         // tensor maps of the FP32 arrays (register-window kernel)
+    long long wait_limit_ = 1LL << 22;        // polls of a bounded mbarrier wait (TMA-staged kernels)
 
     // device buffers
     void* F_[2] = {nullptr, nullptr};

@@ -567,6 +567,11 @@ bool fast3d_supported(const Layout& L, const BlockDev& b, int order) {
     return true;
 }
 
+void launch_faces3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s) {
+    const int nbmax = b.n[2] > b.n[1] ? b.n[2] : b.n[1], namax = b.n[0] > b.n[1] ? b.n[0] : b.n[1];
+    k_faces3d<false><<<dim3((nbmax + 31) / 32, (namax + 3) / 4, 6), dim3(32, 4), 0, s>>>(a, b, sa);
+}
+
 void launch_volume_fast3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s) {
     if (a.cdiss > 0.) {
         launch_volume_exact<float>(a, b, sa, s);   // artificial dissipation: exact-order kernel

@@ -1,0 +1,580 @@
+// Register-window FP32 volume kernel for 3D blocks (volume kernel kind 3).
+//
+// Same discrete operator as the reference's calc_df_3d (src/block.cpp:
+// 1541-2050), outer SAT (src/boundary.cpp:265-503) and RK update
+// (src/fields.cpp:293-309) as the tiled kernel in stage_fast.cu, with the
+// memory traffic organised so that no thread waits on a DRAM load of its own:
+//  * each CTA owns a TJ x TK tile of (j, k) columns of one block and marches
+//    along x through a chunk of planes; two CTAs share an SM;
+//  * every plane's tile data arrives by TMA tensor copies into one of two
+//    shared-memory stages, issued by one thread a plane ahead and counted on
+//    an mbarrier: the centre plane i (fields, metric, Jacobian, rate register)
+//    and the leading plane i+H (fields, x metric row, Jacobian) from which
+//    the x fluxes J (m_x . sigma_c) and velocities enter the x window;
+//  * the x window of the interior stencil (planes i-H .. i+H of the thread's
+//    own column: three fluxes and three velocities each) lives in registers,
+//    so shared memory holds only the two stages and the y/z flux tiles; the
+//    planes near the block's x faces, whose closure rows reach 3H planes,
+//    read their taps straight from global memory;
+//  * the y and z derivative inputs of the centre plane go to shared tiles
+//    with an (order-1) halo; halo nodes are loaded a plane ahead into
+//    registers by the threads that own them;
+//  * interior stencils are unrolled in the antisymmetric form with immediate
+//    coefficients; y closure rows (whole warps) use the tabulated rows and
+//    the two k-edge tiles use one tap row per lane, as in stage_fast.cu;
+//  * nodes on a block face are written without the outer SAT and finished by
+//    the face-node kernel of stage_fast.cu.
+// Each staged box is one tensor copy over a (k, j, i, component) map whose k
+// origin is the 16-byte boundary at or below the tile's first column.  Every
+// mbarrier wait is bounded: on expiry the CTA records FDF_ERR_TIMEOUT, waits
+// (bounded) for the copies it still has in flight and returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <stdexcept>
+
+#include "kernels.hpp"
+#include "sbp_coeffs.cuh"
+#include "stage_common.cuh"
+#include "tma_util.cuh"
+
+namespace fdf {
+
+// tensor maps of the FP32 arrays for kind 3 (F: both field buffers; M9: the
+// nine metric rows; M3: the x metric rows; DF: the rate register)
+struct RegMaps {
+    CUtensorMap F[2], M9, M3, J, DF;
+};
+
+struct RegMapsHost {
+    RegMaps m;
+    const float* F0;
+};
+
+namespace {
+
+constexpr int TJ = 8, TK = 32, NT = TJ * TK;
+constexpr int SW = TK + 4;   // staged row: 16-byte boundary at or below the tile's first column, 36 floats
+
+constexpr int up32(int n) { return (n + 31) / 32 * 32; }   // every box on a 128-byte boundary
+
+template <int ORDER>
+struct RgCfg {
+    static constexpr int H = ORDER - 1, NB = 2 * H, NTB = 3 * H, W = 2 * H + 1;
+    static constexpr int VH = TJ + 2 * H, VW = TK + 2 * H;
+    static constexpr int BOX = TJ * SW;   // floats of one staged component
+    // stage layout, floats: centre F[9], M[9], J, DF[9]; leading F[9], Mx[3], J
+    static constexpr int CF = 0, CM = CF + up32(9 * BOX), CJ = CM + up32(9 * BOX), CD = CJ + up32(BOX),
+                         LF = CD + up32(9 * BOX), LM = LF + up32(9 * BOX), LJ = LM + up32(3 * BOX),
+                         SSZ = LJ + up32(BOX);
+    static constexpr uint32_t BYTES = 4u * 41 * BOX;
+    static constexpr int TY = 3 * VH * TK, TZ = 3 * TJ * VW;   // float2
+    static constexpr int WROWS = 2 * NB + 1;
+    static constexpr int WTAB = ((WROWS * NTB + 3) / 4) * 4;
+    static constexpr size_t SMEM =
+        sizeof(float) * 2 * SSZ + sizeof(float2) * (TY + TZ) + sizeof(float) * WTAB + 2 * sizeof(uint64_t);
+};
+
+template <int ORDER>
+__device__ __forceinline__ constexpr float inner_c(int n) {
+    return ORDER == 4 ? (n == 1 ? 0.75f : (n == 2 ? -0.15f : 1.f / 60.f))
+                      : (ORDER == 3 ? (n == 1 ? 2.f / 3.f : -1.f / 12.f) : 0.5f);
+}
+
+__device__ __forceinline__ void fluxes(float J, float m0, float m1, float m2, const float s[6], float F[3]) {
+    F[0] = J * (m0 * s[0] + m1 * s[1] + m2 * s[2]);
+    F[1] = J * (m0 * s[1] + m1 * s[3] + m2 * s[4]);
+    F[2] = J * (m0 * s[2] + m1 * s[4] + m2 * s[5]);
+}
+
+struct HaloNode {
+    float s[6], v[3], m[3], J;
+};
+
+template <int ORDER>
+__global__ void __launch_bounds__(NT, 2)
+    k_reg3d(VolumeArgs<float> a, BlockDev B, StageArgs sa, int chunk, int* status,
+            const __grid_constant__ RegMaps maps, int fsel) {
+    using C = RgCfg<ORDER>;
+    constexpr int H = C::H, NB = C::NB, NTB = C::NTB, W = C::W, VH = C::VH, VW = C::VW, BOX = C::BOX;
+    extern __shared__ __align__(128) float smem[];
+    float* stg = smem;                                            // two stages of C::SSZ floats
+    float2* ty = reinterpret_cast<float2*>(smem + 2 * C::SSZ);   // [3][VH][TK]  (F_y,c , v_c)
+    float2* tz = ty + C::TY;                                     // [3][TJ][VW]  (F_z,c , v_c)
+    float* wtab = reinterpret_cast<float*>(tz + C::TZ);          // [WROWS][NTB]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(wtab + C::WTAB);
+
+    const Layout& L = a.L;
+    const int cs = (int)L.cstride;
+    const int n0 = B.n[0], n1 = B.n[1], n2 = B.n[2];
+    const int tid = threadIdx.x;
+    const int tk = tid % TK, tj = tid / TK;
+    // tiles and ownership as in stage_fast.cu: the last tile in j and k ends
+    // on the block face and owns the closure rows near it
+    const bool lastk = blockIdx.x == gridDim.x - 1, lastj = blockIdx.y == gridDim.y - 1;
+    const int k0 = lastk ? n2 - TK : blockIdx.x * TK;
+    const int j0 = lastj ? n1 - TJ : blockIdx.y * TJ;
+    const int k = k0 + tk, j = j0 + tj;
+    const bool ownk = (k >= n2 - NB) ? lastk : (k / TK == (int)blockIdx.x);
+    const bool ownj = (j >= n1 - NB) ? lastj : (j / TJ == (int)blockIdx.y);
+    const bool owner = ownk && ownj;
+    const int ib = blockIdx.z * chunk;
+    const int ie = min(n0, ib + chunk);
+    if (ib >= ie) return;
+    const long long wlim = sa.wait_limit > 0 ? sa.wait_limit : (1LL << 22);
+
+    // staged boxes: k origin at the 16-byte boundary at or below the tile
+    const int kg = B.lo[2] + k0;
+    const int kofs = kg & 3;
+    const int kgb = kg - kofs;
+    const int jg = B.lo[1] + j0;
+    const CUtensorMap* mF = &maps.F[fsel];
+    const uint32_t bar0 = saddr(bars), bar1 = saddr(bars + 1);
+
+    const bool kedge = (blockIdx.x == 0) || lastk;
+    if (tid == 0) {
+        bar_init(bar0);
+        bar_init(bar1);
+        bar_init_fence();
+    }
+    if (kedge && tid < C::WROWS * NTB) {
+        const int r = tid / NTB, n = tid % NTB;
+        float w;
+        if (r == 0)
+            w = (n <= 2 * H) ? sbp_coef<float>(ORDER, 0, n) : 0.f;
+        else if (r <= NB)
+            w = sbp_coef<float>(ORDER, r, n);
+        else
+            w = -sbp_coef<float>(ORDER, r - NB, n);
+        wtab[tid] = w;
+    }
+    __syncthreads();
+
+    // one thread: centre plane i and leading plane i+H into stage b
+    auto issue = [&](int i, int b) {
+        float* st = stg + b * C::SSZ;
+        const uint32_t bar = b ? bar1 : bar0;
+        const int ig = B.lo[0] + i;
+        fence_proxy_async();
+        bar_expect(bar, C::BYTES);
+        tma4(saddr(st + C::CF), mF, kgb, jg, ig, 0, bar);
+        tma4(saddr(st + C::CM), &maps.M9, kgb, jg, ig, 0, bar);
+        tma3(saddr(st + C::CJ), &maps.J, kgb, jg, ig, bar);
+        tma4(saddr(st + C::CD), &maps.DF, kgb, jg, ig, 0, bar);
+        tma4(saddr(st + C::LF), mF, kgb, jg, ig + H, 0, bar);
+        tma4(saddr(st + C::LM), &maps.M3, kgb, jg, ig + H, 0, bar);
+        tma3(saddr(st + C::LJ), &maps.J, kgb, jg, ig + H, bar);
+    };
+    if (tid == 0) {
+        issue(ib, 0);
+        if (ib + 1 < ie) issue(ib + 1, 1);
+    }
+    int issued = min(ie, ib + 2);   // planes whose stage was issued (uniform over the CTA)
+
+    // this lane's k-edge row: tap n reads column kb + ks * min(n, kmax) of its tz row
+    int kb = tk, ks = 1, kmax = 2 * H, kw = 0;
+    if (ownk && k < NB) {
+        kb = H - k0;
+        kmax = NTB - 1;
+        kw = (k + 1) * NTB;
+    } else if (ownk && k >= n2 - NB) {
+        kb = (n2 - 1 - k0) + H;
+        ks = -1;
+        kmax = NTB - 1;
+        kw = (NB + n2 - k) * NTB;
+    }
+
+    const int s0 = (int)L.s0;
+    const int colbase = B.lo[0] * s0 + (B.lo[1] + j) * (int)L.s1 + (B.lo[2] + k);
+    const float* __restrict__ F = a.F;
+    const float* __restrict__ M = a.M;
+    const float* __restrict__ Jg = a.J;
+    float* __restrict__ DFg = a.DF;
+    float* __restrict__ Fn = a.Fn;
+
+    // halo node handled by this thread (fixed for the whole march)
+    int hj = 0, hk = 0, hkind = -1;   // 0: j-halo (F_y), 1: k-halo (F_z)
+    if (tid < 2 * H * (TK + TJ)) {
+        if (tid < 2 * H * TK) {
+            const int r = tid / TK, c = tid % TK;
+            hj = (r < H) ? (r - H) : (TJ + r - H);
+            hk = c;
+            hkind = 0;
+        } else {
+            const int t2 = tid - 2 * H * TK;
+            const int r = t2 / (2 * H), c = t2 % (2 * H);
+            hj = r;
+            hk = (c < H) ? (c - H) : (TK + c - H);
+            hkind = 1;
+        }
+        const int gj = j0 + hj, gk = k0 + hk;
+        if (gj < 0 || gj >= n1 || gk < 0 || gk >= n2) hkind = -1;
+    }
+    const int hbase = B.lo[0] * s0 + (B.lo[1] + j0 + hj) * (int)L.s1 + (B.lo[2] + k0 + hk);
+    const int hrow = (hkind == 0) ? 3 : 6;   // metric row y or z
+    auto load_halo = [&](int i, HaloNode& h) {
+        if (hkind < 0) return;
+        const int id = hbase + i * s0;
+#pragma unroll
+        for (int c = 0; c < 6; c++) h.s[c] = __ldg(F + (3 + c) * cs + id);
+#pragma unroll
+        for (int c = 0; c < 3; c++) h.v[c] = __ldg(F + c * cs + id);
+#pragma unroll
+        for (int c = 0; c < 3; c++) h.m[c] = __ldg(M + (hrow + c) * cs + id);
+        h.J = __ldg(Jg + id);
+    };
+    // x flux and velocity of this thread's column at plane q, from global memory
+    auto direct = [&](int q, float Fx[3], float v[3]) {
+        const int id = colbase + q * s0;
+        float s[6];
+#pragma unroll
+        for (int c = 0; c < 6; c++) s[c] = __ldg(F + (3 + c) * cs + id);
+#pragma unroll
+        for (int c = 0; c < 3; c++) v[c] = __ldg(F + c * cs + id);
+        fluxes(__ldg(Jg + id), __ldg(M + id), __ldg(M + cs + id), __ldg(M + 2 * cs + id), s, Fx);
+    };
+
+    float crho[3], sd[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        crho[d] = (float)B.coef[d][0];
+        sd[d] = (float)(sa.dt / B.dx[d]);
+    }
+    const float lamc = (float)B.lam, gc = (float)B.g, g2c = (float)(2. * B.g);
+    const float Acoef = (float)sa.A, Bcoef = (float)sa.B;
+    const bool jint = (j >= NB) && (j < n1 - NB);
+    const bool face = (j == 0) | (j == n1 - 1) | (k == 0) | (k == n2 - 1);
+
+    // x window: after the insert at plane i, wF/wv[m] hold plane i - H + m.
+    // A chunk that starts past the left closure rows fills planes ib-H..ib+H-1
+    // from global memory; the first chunk builds its window from the inserts.
+    float wF[W][3], wv[W][3];
+#pragma unroll
+    for (int m = 0; m < W; m++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) wF[m][c] = wv[m][c] = 0.f;
+    if (ib >= NB && ib < n0 - NB) {
+#pragma unroll
+        for (int m = 1; m < W; m++) direct(ib - H - 1 + m, wF[m], wv[m]);
+    }
+    HaloNode hn;
+    load_halo(ib, hn);
+
+    const int so = tj * SW + tk + kofs;   // this node in a staged component
+    for (int i = ib; i < ie; i++) {
+        const int b = (i - ib) & 1;
+        const float* st = stg + b * C::SSZ;
+        const bool ok = bar_wait(b ? bar1 : bar0, ((i - ib) >> 1) & 1, wlim);
+        // ---- leading plane i+H enters the x window
+        if (i + H < n0) {
+            float s[6], v[3], Fx[3];
+#pragma unroll
+            for (int c = 0; c < 6; c++) s[c] = st[C::LF + (3 + c) * BOX + so];
+#pragma unroll
+            for (int c = 0; c < 3; c++) v[c] = st[C::LF + c * BOX + so];
+            fluxes(st[C::LJ + so], st[C::LM + so], st[C::LM + BOX + so], st[C::LM + 2 * BOX + so], s, Fx);
+#pragma unroll
+            for (int m = 0; m < W - 1; m++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    wF[m][c] = wF[m + 1][c];
+                    wv[m][c] = wv[m + 1][c];
+                }
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                wF[W - 1][c] = Fx[c];
+                wv[W - 1][c] = v[c];
+            }
+        }
+        // ---- centre plane i: y/z flux tiles of the tile and of this thread's halo node
+        {
+            float s[6], Fy[3], Fz[3];
+#pragma unroll
+            for (int c = 0; c < 6; c++) s[c] = st[C::CF + (3 + c) * BOX + so];
+            const float Jc = st[C::CJ + so];
+            fluxes(Jc, st[C::CM + 3 * BOX + so], st[C::CM + 4 * BOX + so], st[C::CM + 5 * BOX + so], s, Fy);
+            fluxes(Jc, st[C::CM + 6 * BOX + so], st[C::CM + 7 * BOX + so], st[C::CM + 8 * BOX + so], s, Fz);
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const float v = st[C::CF + c * BOX + so];
+                ty[(c * VH + tj + H) * TK + tk] = make_float2(Fy[c], v);
+                tz[(c * TJ + tj) * VW + tk + H] = make_float2(Fz[c], v);
+            }
+        }
+        if (hkind >= 0) {
+            float Fh[3];
+            fluxes(hn.J, hn.m[0], hn.m[1], hn.m[2], hn.s, Fh);
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                if (hkind == 0)
+                    ty[(c * VH + hj + H) * TK + hk] = make_float2(Fh[c], hn.v[c]);
+                else
+                    tz[(c * TJ + hj) * VW + hk + H] = make_float2(Fh[c], hn.v[c]);
+            }
+        }
+        if (i + 1 < ie) load_halo(i + 1, hn);
+        if (__syncthreads_or(!ok)) {   // flux tiles ready; every thread is done with plane i-1's stage
+            if (tid == 0) {
+                atomicOr(status, FDF_ERR_TIMEOUT);
+                // wait for the copies still in flight before the CTA leaves
+                for (int q = i; q < issued; q++)
+                    bar_wait((q - ib) & 1 ? bar1 : bar0, ((q - ib) >> 1) & 1, TMA_DRAIN_LIMIT);
+            }
+            return;
+        }
+        if (i > ib && issued < ie) {   // plane i+1 into the stage plane i-1 used
+            if (tid == 0) issue(issued, (issued - ib) & 1);
+            issued++;
+        }
+
+        // ---- derivatives: DFl[d][c] of the fluxes, Dv[d][c] of the velocities
+        float DFl[3][3], Dv[3][3];
+        if (i >= NB && i < n0 - NB) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                float af = 0.f, av = 0.f;
+#pragma unroll
+                for (int n = 1; n <= H; n++) {
+                    af = fmaf(inner_c<ORDER>(n), wF[H + n][c] - wF[H - n][c], af);
+                    av = fmaf(inner_c<ORDER>(n), wv[H + n][c] - wv[H - n][c], av);
+                }
+                DFl[0][c] = af;
+                Dv[0][c] = av;
+            }
+        } else {   // x closure rows: 3H taps from global memory
+            const bool left = i < NB;
+            const int row = left ? i + 1 : n0 - i;
+            const float sg = left ? 1.f : -1.f;
+            float af[3] = {0.f, 0.f, 0.f}, av[3] = {0.f, 0.f, 0.f};
+            for (int n = 0; n < NTB; n++) {
+                const float cf = sbp_coef<float>(ORDER, row, n);
+                float Fx[3], v[3];
+                direct(left ? n : n0 - 1 - n, Fx, v);
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    af[c] = fmaf(cf, Fx[c], af[c]);
+                    av[c] = fmaf(cf, v[c], av[c]);
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                DFl[0][c] = sg * af[c];
+                Dv[0][c] = sg * av[c];
+            }
+        }
+        // closure rows this tile does not write may have taps outside the tile:
+        // they take the interior form (taps in the tile and its halo), discarded
+        const bool jskip = !jint && !ownj;
+        if (jint || jskip) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                float af = 0.f, av = 0.f;
+#pragma unroll
+                for (int n = 1; n <= H; n++) {
+                    const float2 p = ty[(c * VH + tj + H + n) * TK + tk];
+                    const float2 q = ty[(c * VH + tj + H - n) * TK + tk];
+                    af = fmaf(inner_c<ORDER>(n), p.x - q.x, af);
+                    av = fmaf(inner_c<ORDER>(n), p.y - q.y, av);
+                }
+                DFl[1][c] = af;
+                Dv[1][c] = av;
+            }
+        } else {
+            const bool left = j < NB;
+            const int row = left ? j + 1 : n1 - j;
+            const int base = (left ? 0 : n1 - 1) - j0 + H, step = left ? 1 : -1;
+            const float sg = left ? 1.f : -1.f;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                float af = 0.f, av = 0.f;
+                for (int n = 0; n < NTB; n++) {
+                    const float cf = sbp_coef<float>(ORDER, row, n);
+                    const float2 p = ty[(c * VH + base + n * step) * TK + tk];
+                    af = fmaf(cf, p.x, af);
+                    av = fmaf(cf, p.y, av);
+                }
+                DFl[1][c] = sg * af;
+                Dv[1][c] = sg * av;
+            }
+        }
+        if (!kedge) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                float af = 0.f, av = 0.f;
+#pragma unroll
+                for (int n = 1; n <= H; n++) {
+                    const float2 p = tz[(c * TJ + tj) * VW + tk + H + n];
+                    const float2 q = tz[(c * TJ + tj) * VW + tk + H - n];
+                    af = fmaf(inner_c<ORDER>(n), p.x - q.x, af);
+                    av = fmaf(inner_c<ORDER>(n), p.y - q.y, av);
+                }
+                DFl[2][c] = af;
+                Dv[2][c] = av;
+            }
+        } else {
+            float af[3] = {0.f, 0.f, 0.f}, av[3] = {0.f, 0.f, 0.f};
+            const float2* trow = tz + tj * VW;
+#pragma unroll
+            for (int n = 0; n < NTB; n++) {
+                const float w = wtab[kw + n];
+                const int col = kb + ks * min(n, kmax);
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const float2 p = trow[c * TJ * VW + col];
+                    af[c] = fmaf(w, p.x, af[c]);
+                    av[c] = fmaf(w, p.y, av[c]);
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                DFl[2][c] = af[c];
+                Dv[2][c] = av[c];
+            }
+        }
+        __syncthreads();   // flux tiles are rewritten for the next plane
+
+        // ---- rate: df = A df + L(f), then the RK update
+        float df[9];
+#pragma unroll
+        for (int c = 0; c < 9; c++) df[c] = st[C::CD + c * BOX + so];
+        const float iJ = __frcp_rn(st[C::CJ + so]);
+        {
+            const float w0 = crho[0] * iJ, w1 = crho[1] * iJ, w2 = crho[2] * iJ;
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+                df[c] = fmaf(w2, DFl[2][c], fmaf(w1, DFl[1][c], fmaf(w0, DFl[0][c], Acoef * df[c])));
+        }
+        {
+            // velocity gradient e[a][b] = d v_a / d x_b (times dt)
+#pragma unroll
+            for (int d = 0; d < 3; d++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) Dv[d][c] *= sd[d];
+            float m[9];
+#pragma unroll
+            for (int c = 0; c < 9; c++) m[c] = st[C::CM + c * BOX + so];
+            float e[3][3];
+#pragma unroll
+            for (int va = 0; va < 3; va++)
+#pragma unroll
+                for (int bb = 0; bb < 3; bb++)
+                    e[va][bb] = fmaf(m[6 + bb], Dv[2][va], fmaf(m[3 + bb], Dv[1][va], m[bb] * Dv[0][va]));
+            const float lt = lamc * (e[0][0] + e[1][1] + e[2][2]);
+            df[3] = fmaf(Acoef, df[3], fmaf(g2c, e[0][0], lt));
+            df[4] = fmaf(Acoef, df[4], gc * (e[0][1] + e[1][0]));
+            df[5] = fmaf(Acoef, df[5], gc * (e[0][2] + e[2][0]));
+            df[6] = fmaf(Acoef, df[6], fmaf(g2c, e[1][1], lt));
+            df[7] = fmaf(Acoef, df[7], gc * (e[1][2] + e[2][1]));
+            df[8] = fmaf(Acoef, df[8], fmaf(g2c, e[2][2], lt));
+        }
+        if (owner) {
+            const int id = colbase + i * s0;
+#pragma unroll
+            for (int c = 0; c < 9; c++) DFg[c * cs + id] = df[c];
+            // face nodes: k_faces3d adds the outer SATs and finishes them
+            if (!(face | (i == 0) | (i == n0 - 1))) {
+#pragma unroll
+                for (int c = 0; c < 9; c++) Fn[c * cs + id] = fmaf(Bcoef, df[c], st[C::CF + c * BOX + so]);
+            }
+        }
+    }
+}
+
+// choose the x chunk: the grid of tiles x chunks runs in whole waves of
+// `slots` resident CTAs; each chunk also pays about H planes of window set-up
+int pick_chunk(int n0, int tiles, int slots, int H) {
+    int best = n0, bestcost = 1 << 30;
+    for (int chunks = 1; chunks <= 64; chunks++) {
+        const int chunk = (n0 + chunks - 1) / chunks;
+        if (chunk < 16 && chunks > 1) break;
+        const int nc = (n0 + chunk - 1) / chunk;
+        const int waves = (tiles * nc + slots - 1) / slots;
+        const int cost = waves * (chunk + H + 1);
+        if (cost < bestcost) {
+            bestcost = cost;
+            best = chunk;
+        }
+    }
+    return best;
+}
+
+template <int ORDER>
+void launch_order(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, int* status,
+                  const RegMapsHost& mh, cudaStream_t s) {
+    using C = RgCfg<ORDER>;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    // the shared-memory opt-in is a per-device function attribute: set it once per device
+    static std::atomic<unsigned> configured{0};
+    static int occ[32] = {0};
+    const unsigned bit = 1u << (dev & 31);
+    if (!(configured.load() & bit)) {
+        cudaFuncSetAttribute(k_reg3d<ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+        int o = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_reg3d<ORDER>, NT, C::SMEM);
+        occ[dev & 31] = o > 0 ? o : 1;
+        configured.fetch_or(bit);
+    }
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int tk = (b.n[2] + TK - 1) / TK, tj = (b.n[1] + TJ - 1) / TJ;
+    const int chunk = pick_chunk(b.n[0], tk * tj, occ[dev & 31] * nsm, ORDER - 1);
+    const int chunks = (b.n[0] + chunk - 1) / chunk;
+    dim3 grid(tk, tj, chunks);
+    const int fsel = (a.F == mh.F0) ? 0 : 1;
+    k_reg3d<ORDER><<<grid, NT, C::SMEM, s>>>(a, b, sa, chunk, status, mh.m, fsel);
+    launch_faces3d(a, b, sa, s);
+}
+
+}  // namespace
+
+RegMapsHost* make_reg_maps(const Layout& L, const float* F0, const float* F1, const float* M, const float* J,
+                           const float* DF) {
+    RegMapsHost* h = new RegMapsHost;
+    h->F0 = F0;
+    const cuuint64_t d4[4] = {(cuuint64_t)L.s1, (cuuint64_t)L.nx[1], (cuuint64_t)L.nx[0], 9};
+    const cuuint64_t s4[3] = {(cuuint64_t)L.s1 * 4, (cuuint64_t)L.s0 * 4, (cuuint64_t)L.cstride * 4};
+    const cuuint64_t d3[3] = {(cuuint64_t)L.s1, (cuuint64_t)L.nx[1], (cuuint64_t)L.nx[0]};
+    const cuuint32_t b9[4] = {SW, TJ, 1, 9}, b3[4] = {SW, TJ, 1, 3}, b1[3] = {SW, TJ, 1};
+    try {
+        tma_encode(&h->m.F[0], F0, 4, d4, s4, b9);
+        tma_encode(&h->m.F[1], F1, 4, d4, s4, b9);
+        tma_encode(&h->m.M9, M, 4, d4, s4, b9);
+        tma_encode(&h->m.M3, M, 4, d4, s4, b3);
+        tma_encode(&h->m.J, J, 3, d3, s4, b1);
+        tma_encode(&h->m.DF, DF, 4, d4, s4, b9);
+    } catch (...) {
+        delete h;
+        throw;
+    }
+    return h;
+}
+
+void free_reg_maps(RegMapsHost* h) { delete h; }
+
+bool reg3d_supported(const Layout& L, const BlockDev& b, int order) {
+    if (L.ndim != 3 || L.nfields != 9) return false;
+    if (order < 2 || order > 4) return false;
+    if (b.n[1] < TJ || b.n[2] < TK) return false;
+    if (b.n[0] < 4 * order - 3) return false;
+    if (L.cstride * 9 >= (1LL << 31)) return false;   // 32-bit element offsets
+    if (L.s1 % 4 != 0 || L.s0 % 4 != 0 || L.cstride % 4 != 0) return false;   // 16-byte row starts
+    return true;
+}
+
+void launch_volume_reg3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, int* status,
+                         const RegMapsHost* maps, cudaStream_t s) {
+    if (a.cdiss > 0. || sa.plastic) {   // dissipation / plasticity: the tiled kernel of stage_fast.cu
+        launch_volume_fast3d(a, b, sa, s);
+        return;
+    }
+    if (!maps) throw std::runtime_error("register-window kernel: tensor maps missing");
+    switch (a.order) {
+        case 2: launch_order<2>(a, b, sa, status, *maps, s); break;
+        case 3: launch_order<3>(a, b, sa, status, *maps, s); break;
+        default: launch_order<4>(a, b, sa, status, *maps, s); break;
+    }
+}
+
+}  // namespace fdf

@@ -32,6 +32,7 @@
 #include "kernels.hpp"
 #include "sbp_coeffs.cuh"
 #include "stage_common.cuh"
+#include "tma_util.cuh"
 
 namespace fdf {
 
@@ -54,7 +55,6 @@ namespace {
 constexpr int TJ = 8, TK = 32, NT = TJ * TK;
 constexpr int CW = 44;   // staged centre row, floats: TK + 2H + alignment slack, multiple of 4
 constexpr int RW = 36;   // staged ring row, floats: TK + alignment slack, multiple of 4
-constexpr long long WAIT_LIMIT = 1LL << 22;
 
 constexpr int up32(int n) { return (n + 31) / 32 * 32; }   // 128-byte boundaries for every box
 
@@ -89,43 +89,6 @@ __device__ __forceinline__ void fluxes(float J, float m0, float m1, float m2, co
     F[2] = J * (m0 * s[2] + m1 * s[4] + m2 * s[5]);
 }
 
-__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void bar_init(uint32_t bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(1) : "memory");
-}
-__device__ __forceinline__ void bar_expect(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool bar_try(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
-    for (long long it = 0; it < WAIT_LIMIT; it++)
-        if (bar_try(bar, parity)) return true;
-    return false;
-}
-__device__ __forceinline__ void tma4(uint32_t dst, const CUtensorMap* map, int x, int y, int z, int w, uint32_t bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], "
-        "[%2];\n" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y), "r"(z), "r"(w)
-        : "memory");
-}
-__device__ __forceinline__ void tma3(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
-        "[%2];\n" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y), "r"(z)
-        : "memory");
-}
-
 template <int ORDER>
 __global__ void __launch_bounds__(NT, 1)
     k_tma3d(VolumeArgs<float> a, BlockDev B, StageArgs sa, int chunk, int* status,
@@ -156,6 +119,7 @@ __global__ void __launch_bounds__(NT, 1)
     const int ib = blockIdx.z * chunk;
     const int ie = min(n0, ib + chunk);
     if (ib >= ie) return;
+    const long long wlim = sa.wait_limit > 0 ? sa.wait_limit : (1LL << 22);
 
     const int s0 = (int)L.s0, s1 = (int)L.s1;
     const int colbase = B.lo[0] * s0 + (B.lo[1] + j) * s1 + (B.lo[2] + k);
@@ -178,7 +142,7 @@ __global__ void __launch_bounds__(NT, 1)
     const uint32_t bar_r[2] = {saddr(bars + 2), saddr(bars + 3)};
     if (tid == 0) {
         for (int b = 0; b < 4; b++) bar_init(saddr(bars + b));
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        bar_init_fence();
     }
     __syncthreads();
 
@@ -186,7 +150,7 @@ __global__ void __launch_bounds__(NT, 1)
     auto issue_centre = [&](int q, int b) {
         float* dst = cst0 + b * C::CSZ;
         const int ig = B.lo[0] + q;
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        fence_proxy_async();
         bar_expect(bar_c[b], C::CBYTES);
         tma4(saddr(dst + C::CF), mFc, kgb, jgc, ig, 0, bar_c[b]);
         tma4(saddr(dst + C::CMY), &maps.My, kgb, jgc, ig, 3, bar_c[b]);
@@ -198,7 +162,7 @@ __global__ void __launch_bounds__(NT, 1)
     auto issue_ring = [&](int q, int b) {
         float* dst = rst0 + b * C::RSZ;
         const int ig = B.lo[0] + q;
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        fence_proxy_async();
         bar_expect(bar_r[b], C::RBYTES);
         tma4(saddr(dst), mFr, krs, jgr, ig, 0, bar_r[b]);
         tma4(saddr(dst + C::RMX), &maps.Mr, krs, jgr, ig, 0, bar_r[b]);
@@ -230,10 +194,12 @@ __global__ void __launch_bounds__(NT, 1)
     r_issue = min(q0 + 2, qmax + 1);
     c_issue = min(ib + 2, ie);
 
-    // bounded wait for every copy this CTA still has in flight, before an early exit
-    auto drain = [&](int i_cons) {
-        for (int q = r_cons; q < r_issue; q++) bar_wait(bar_r[(q - q0) & 1], ((q - q0) >> 1) & 1);
-        for (int q = i_cons; q < c_issue; q++) bar_wait(bar_c[(q - ib) & 1], ((q - ib) >> 1) & 1);
+    // bounded wait for every copy this CTA still has in flight, before an early
+    // exit: ring planes from r_first (the one whose wait gave up, if any) and
+    // centre planes from i_cons
+    auto drain = [&](int r_first, int i_cons) {
+        for (int q = r_first; q < r_issue; q++) bar_wait(bar_r[(q - q0) & 1], ((q - q0) >> 1) & 1, TMA_DRAIN_LIMIT);
+        for (int q = i_cons; q < c_issue; q++) bar_wait(bar_c[(q - ib) & 1], ((q - ib) >> 1) & 1, TMA_DRAIN_LIMIT);
     };
 
     int lslot = q0 % R;
@@ -249,7 +215,7 @@ __global__ void __launch_bounds__(NT, 1)
         const int need = maxtap(i);
         while (r_cons <= need) {   // uniform: one plane per iteration in the interior
             const int b = (r_cons - q0) & 1;
-            const bool ok = bar_wait(bar_r[b], ((r_cons - q0) >> 1) & 1);
+            const bool ok = bar_wait(bar_r[b], ((r_cons - q0) >> 1) & 1, wlim);
             const float* rs = rst0 + b * C::RSZ + tj * RW + tk + kofr;
             float s[6], v[3];
 #pragma unroll
@@ -265,7 +231,7 @@ __global__ void __launch_bounds__(NT, 1)
             lslot = (lslot + 1 == R) ? 0 : lslot + 1;
             if (__syncthreads_or(!ok)) {   // staging buffer b is free for the plane two ahead
                 if (tid == 0) atomicOr(status, FDF_ERR_TIMEOUT);
-                drain(i);
+                drain(r_cons - 1, i);   // the plane whose copy may still land, and every later one
                 return;
             }
             if (r_issue <= qmax && r_issue < r_cons + 2) {
@@ -275,7 +241,7 @@ __global__ void __launch_bounds__(NT, 1)
         }
         // ---- centre plane i: flux tiles (tile and halo) and this node's values
         const int cb = (i - ib) & 1;
-        const bool okc = bar_wait(bar_c[cb], ((i - ib) >> 1) & 1);
+        const bool okc = bar_wait(bar_c[cb], ((i - ib) >> 1) & 1, wlim);
         const float* cs_ = cst0 + cb * C::CSZ;
         for (int e = tid; e < VH * TK; e += NT) {   // y fluxes: all VH rows, tile columns
             const int r = e / TK, kk = e % TK;
@@ -316,7 +282,7 @@ __global__ void __launch_bounds__(NT, 1)
         const float Jc = cs_[C::CJ + (tj + H) * CW + tk + H + kofs];
         if (__syncthreads_or(!okc)) {   // flux tiles ready; centre buffer cb free
             if (tid == 0) atomicOr(status, FDF_ERR_TIMEOUT);
-            drain(i);
+            drain(r_cons, i);
             return;
         }
         if (c_issue < ie) {
@@ -532,32 +498,6 @@ void launch_order(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs
     k_tma3d<ORDER><<<grid, NT, C::SMEM, s>>>(a, b, sa, chunk, status, mh.m, fsel);
 }
 
-using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeFn encode_fn() {
-    static EncodeFn fn = nullptr;
-    if (!fn) {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        const cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
-        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p)
-            throw std::runtime_error("CUDA driver entry point cuTensorMapEncodeTiled is unavailable");
-        fn = reinterpret_cast<EncodeFn>(p);
-    }
-    return fn;
-}
-
-void encode(CUtensorMap* m, const float* base, cuuint32_t rank, const cuuint64_t* dims, const cuuint64_t* strides,
-            const cuuint32_t* box) {
-    const cuuint32_t es[4] = {1, 1, 1, 1};
-    const CUresult r = encode_fn()(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, const_cast<float*>(base), dims, strides,
-                                   box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) throw std::runtime_error("CUDA error in cuTensorMapEncodeTiled: " + std::to_string((int)r));
-}
-
 }  // namespace
 
 StagedMapsHost* make_staged_maps(const Layout& L, const float* F0, const float* F1, const float* M, const float* J,
@@ -575,14 +515,14 @@ StagedMapsHost* make_staged_maps(const Layout& L, const float* F0, const float* 
     try {
         const float* F[2] = {F0, F1};
         for (int b = 0; b < 2; b++) {
-            encode(&h->m.Fc[b], F[b], 4, d4, s4, bFc);
-            encode(&h->m.Fr[b], F[b], 4, d4, s4, bFr);
+            tma_encode(&h->m.Fc[b], F[b], 4, d4, s4, bFc);
+            tma_encode(&h->m.Fr[b], F[b], 4, d4, s4, bFr);
         }
-        encode(&h->m.My, M, 4, d4, s4, bMy);
-        encode(&h->m.Mt, M, 4, d4, s4, bMt);
-        encode(&h->m.Mr, M, 4, d4, s4, bMr);
-        encode(&h->m.Jc, J, 3, d3, s4, bJc);
-        encode(&h->m.Jr, J, 3, d3, s4, bJr);
+        tma_encode(&h->m.My, M, 4, d4, s4, bMy);
+        tma_encode(&h->m.Mt, M, 4, d4, s4, bMt);
+        tma_encode(&h->m.Mr, M, 4, d4, s4, bMr);
+        tma_encode(&h->m.Jc, J, 3, d3, s4, bJc);
+        tma_encode(&h->m.Jr, J, 3, d3, s4, bJr);
     } catch (...) {
         delete h;
         throw;

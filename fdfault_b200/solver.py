@@ -69,6 +69,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fdf_profile_read.argtypes = [ctypes.c_void_p, c_int, dp, P(c_ll)]
     L.fdf_use_fast_kernel.argtypes = [ctypes.c_void_p, c_int, P(c_int)]
     L.fdf_set_volume_kernel.argtypes = [ctypes.c_void_p, c_int, P(c_int)]
+    L.fdf_set_wait_limit.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
     L.fdf_use_graphs.argtypes = [ctypes.c_void_p, c_int]
     L.fdf_bytes_per_node_stage.argtypes = [ctypes.c_void_p, P(c_ll)]
     fp = P(ctypes.c_float)
@@ -130,6 +131,7 @@ class Problem:
         self._h = h
         self._owner = _owner
         self.precision = precision
+        self.device = device
         ints = (ctypes.c_int * 16)()
         dbls = (ctypes.c_double * 3)()
         self._check(self._L.fdf_get_info(self._h, ints, dbls))
@@ -271,11 +273,16 @@ class Problem:
         self._check(self._L.fdf_use_graphs(self._h, int(on)))
 
     def set_volume_kernel(self, kind: int) -> int:
-        """FP32 volume kernel: 0 reference order, 1 tiled (3D, or 2D elastic), 2 staged (3D);
-        returns the kind that runs."""
+        """FP32 volume kernel: 0 reference order, 1 tiled (3D, or 2D elastic), 2 staged (3D),
+        3 register window (3D); returns the kind that runs."""
         act = ctypes.c_int()
         self._check(self._L.fdf_set_volume_kernel(self._h, kind, ctypes.byref(act)))
         return act.value
+
+    def set_wait_limit(self, polls: int) -> None:
+        """Polls of each bounded wait for staged data in volume kernels 2 and 3
+        (<= 0: the built-in limit); 1 makes every wait a single immediate test."""
+        self._check(self._L.fdf_set_wait_limit(self._h, polls))
 
     def use_fast_kernel(self, on: bool) -> bool:
         act = ctypes.c_int()
@@ -352,6 +359,7 @@ class Ensemble:
         if rc:
             raise FdfaultError(self._L.fdf_ensemble_last_error(None).decode())
         self._h = h
+        self.device = device
         self._members = {}
         n = ctypes.c_int()
         self._check(self._L.fdf_ensemble_size(self._h, ctypes.byref(n)))
@@ -365,7 +373,7 @@ class Ensemble:
         if i not in self._members:
             h = ctypes.c_void_p()
             self._check(self._L.fdf_ensemble_member(self._h, i, ctypes.byref(h)))
-            self._members[i] = Problem(None, FP32, _handle=h, _owner=self)
+            self._members[i] = Problem(None, FP32, device=self.device, _handle=h, _owner=self)
         return self._members[i]
 
     def run(self, nsteps: int) -> None:

@@ -147,10 +147,23 @@ int fdf_use_fast_kernel(fdf_handle* h, int on, int* active);
 /* FP32 volume kernel by kind: 0 one thread per node (reference operation
  * order), 1 tiled (the default: 3D blocks of at least 8 x 32 in y x z, and 2D
  * elastic blocks at least 32 nodes wide in y), 2 staged (3D only: planes
- * brought into shared memory by TMA tensor copies).  active = the kind that
+ * brought into shared memory by TMA tensor copies), 3 register window (3D
+ * only, same block sizes as kind 1: the x stencil window in registers, every
+ * plane of a tile staged by TMA tensor copies; plastic or dissipative stages
+ * run kind 1).  active = the kind that
  * will run (0 where the chosen one does not apply to the problem; FP64
  * problems always run kind 0). */
 int fdf_set_volume_kernel(fdf_handle* h, int kind, int* active);
+
+/* Polls of each bounded wait for staged data in the TMA-staged volume kernels
+ * (kinds 2 and 3); polls <= 0 restores the built-in limit (2^22).  A wait that
+ * runs out makes its CTA record FDF_ERR_TIMEOUT in the device status word
+ * (reported by the next fdf_synchronize as FDF_ERR_SOLVER), wait with a fixed
+ * generous limit for its own copies still in flight, and return; the fields of
+ * that stage are then incomplete.  With polls = 1 every wait is a single
+ * immediate test, which lets a test exercise this path.  No reference
+ * counterpart: the reference has no device waits. */
+int fdf_set_wait_limit(fdf_handle* h, long long polls);
 
 /* Algorithmic bytes moved per node per stage by the volume kernel. */
 int fdf_bytes_per_node_stage(fdf_handle* h, long long* bytes);

@@ -57,7 +57,7 @@ CASES = {
 
 def stage_from_random_state(infile, kind, seed=21):
     """Fields and rates after each stage of one step from a seeded random state,
-    with volume kernel `kind` (0 reference order, 1 tiled, 2 staged)."""
+    with volume kernel `kind` (0 reference order, 1 tiled, 2 staged, 3 register window)."""
     rng = np.random.default_rng(seed)
     out = []
     with fs.Problem(infile, precision=fs.FP32) as p:
@@ -72,7 +72,7 @@ def stage_from_random_state(infile, kind, seed=21):
     return active, out
 
 
-@pytest.mark.parametrize("kind", [1, 2])
+@pytest.mark.parametrize("kind", [1, 2, 3])
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_fast_kernel_matches_reference_order_kernel(name, kind, tmp_path):
     """Same operator: one step from a random state agrees to FP32 rounding
@@ -88,7 +88,7 @@ def test_fast_kernel_matches_reference_order_kernel(name, kind, tmp_path):
             assert e < 1e-5, (s, k, e)
 
 
-@pytest.mark.parametrize("kind", [1, 2])
+@pytest.mark.parametrize("kind", [1, 2, 3])
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_fast_kernel_rupture_close_to_fp64(name, kind, tmp_path):
     """A rupture run with the tiled or staged kernel stays within the FP32 tolerance of the FP64 oracle."""

@@ -81,3 +81,24 @@ def test_noalloc_rejects_oversize():
             p.field_noalloc(0)
         # the handle stays usable after the rejection
         assert np.isfinite(p.field(0)).all()
+
+
+def test_noalloc_reserves_nothing_after_set_up():
+    """The static buffer is reserved when a handle is created, so the first
+    allocation-free calls of a fresh handle change the device's free memory by
+    nothing."""
+    import torch
+
+    tmp = tempfile.mkdtemp(prefix="fdf_noalloc_")
+    prob = P.mode2_rupture(nx=61, ny=31, h=0.1, nt=4, name="na_fresh", datadir=tmp + "/", nuc_half=1.0)
+    infile = prob.write(os.path.join(tmp, "na_fresh.in"))
+    torch.cuda.init()
+    with fs.Problem(infile, precision=fs.FP64) as p:
+        p.step(2)
+        p.synchronize()
+        free0 = torch.cuda.mem_get_info(p.device)[0]
+        for comp in range(p.nfields):
+            p.field_noalloc(comp)
+            p.field_noalloc(comp, True)
+        p.synchronize()
+        assert torch.cuda.mem_get_info(p.device)[0] == free0
