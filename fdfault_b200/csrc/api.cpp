@@ -52,6 +52,24 @@ class DeviceGuard {
     bool changed_ = false;
 };
 
+// Restores the caller's current device on exit (construction sets the new
+// handle's device itself, after the input has been read and checked).
+class DeviceRestore {
+  public:
+    DeviceRestore() {
+        if (cudaGetDevice(&prev_) != cudaSuccess) prev_ = -1;
+    }
+    ~DeviceRestore() {
+        int now = -1;
+        if (prev_ >= 0 && cudaGetDevice(&now) == cudaSuccess && now != prev_) cudaSetDevice(prev_);
+    }
+    DeviceRestore(const DeviceRestore&) = delete;
+    DeviceRestore& operator=(const DeviceRestore&) = delete;
+
+  private:
+    int prev_ = -1;
+};
+
 template <typename F>
 int guarded(fdf_handle* h, F&& f) {
     if (!h || !h->s) return FDF_ERR_ARG;
@@ -93,7 +111,7 @@ int fdf_create(const char* infile, int precision, int device, fdf_handle** out) 
     try {
         fdf_handle* h = new fdf_handle;
         try {
-            DeviceGuard dg(device);   // the caller's current device is restored on return
+            DeviceRestore dr;   // the caller's current device is restored on return
             h->s = new fdf::Solver(infile, precision, device);
         } catch (...) {
             delete h;
@@ -344,7 +362,7 @@ int fdf_ensemble_create(const char* const* infiles, int n, int device, fdf_ensem
         }
         fdf_ensemble* h = new fdf_ensemble;
         try {
-            DeviceGuard dg(device);   // the caller's current device is restored on return
+            DeviceRestore dr;   // the caller's current device is restored on return
             h->e = new fdf::Ensemble(files, device);
         } catch (...) {
             delete h;
