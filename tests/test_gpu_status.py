@@ -30,19 +30,36 @@ def status_bits(err):
 
 
 @pytest.mark.parametrize("precision", [fs.FP64, fs.FP32])
-def test_nan_in_load_file_is_reported(tmp_path, precision):
+def test_nan_in_load_file_is_reported_at_set_up(tmp_path, precision):
+    """A NaN in a load file reaches the initial interface solve: creation fails
+    with the non-finite bit in its message."""
     prob = build_case("m2_files", str(tmp_path), outputs=False)
     lf = prob.interfaces[0].loadfile
     loads = np.fromfile(lf, dtype="<f8").reshape(3, -1)
     loads[:, 30] = np.nan
     loads.astype("<f8").tofile(lf)
     infile = prob.write(os.path.join(str(tmp_path), prob.name + ".in"))
+    with pytest.raises(fs.FdfaultError) as ei:
+        fs.Problem(infile, precision=precision)
+    m = re.search(r"status (\d+)", str(ei.value))
+    assert m and int(m.group(1)) & ERR_NONFINITE, str(ei.value)
+
+
+@pytest.mark.parametrize("precision", [fs.FP64, fs.FP32])
+def test_nan_in_fields_is_reported_by_synchronize(tmp_path, precision):
+    """A NaN put into the fields after set-up is found by the interface kernel
+    during stepping and reported by fdf_synchronize; the word is cleared once
+    read and the handle stays usable."""
+    prob = build_case("m2_sw", str(tmp_path), outputs=False)
+    infile = prob.write(os.path.join(str(tmp_path), prob.name + ".in"))
     with fs.Problem(infile, precision=precision) as p:
-        p.step(2)
+        p.step(1)
+        p.synchronize()
+        p.set_field(0, np.full(p.nxyz, np.nan))
+        p.step(1)
         with pytest.raises(fs.FdfaultError) as ei:
             p.synchronize()
         assert status_bits(ei.value) & ERR_NONFINITE
-        # the status word is cleared once read; the handle stays usable
         p.set_field(0, np.zeros(p.nxyz))
         assert np.all(p.field(0) == 0.0)
         p.synchronize()
