@@ -77,15 +77,17 @@ void launch_volume_staged3d(const VolumeArgs<float>& a, const BlockDev& b, const
 bool staged3d_supported(const Layout& L, const BlockDev& b, int order);
 // register-window FP32 3D kernel (x window in registers, tile planes staged by TMA)
 struct RegMapsHost;
+// (allocates, per block, the k-face SAT increment buffer of 18 x n0 x n1 floats)
 RegMapsHost* make_reg_maps(const Layout& L, const float* F0, const float* F1, const float* M, const float* J,
-                           const float* DF);
+                           const float* DF, const BlockDev* blocks, int nblocks);
 void free_reg_maps(RegMapsHost* h);
-void launch_volume_reg3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, int* status,
+void launch_volume_reg3d(const VolumeArgs<float>& a, const BlockDev& b, int bi, const StageArgs& sa, int* status,
                          const RegMapsHost* maps, cudaStream_t s);
 bool reg3d_supported(const Layout& L, const BlockDev& b, int order);
 // outer SATs and RK update of the face nodes of a 3D block (elastic), after a
-// marching kernel wrote their rate without the SAT
-void launch_faces3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s);
+// marching kernel wrote their rate without the SAT (kdone: the k-face SATs are
+// already in the rate and nodes on k faces only are finished)
+void launch_faces3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, bool kdone, cudaStream_t s);
 
 // interface kernels
 template <typename T>

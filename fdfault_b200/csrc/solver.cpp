@@ -854,8 +854,8 @@ void Solver::stage_impl(double dt, int stage, double t, bool for_step) {
             } else if (vk == 3) {
                 if (!reg_maps_)
                     reg_maps_ = make_reg_maps(L_, (const float*)F_[0], (const float*)F_[1], (const float*)M_,
-                                              (const float*)J_, (const float*)DF_);
-                launch_volume_reg3d(va, blocks_[b], sa, status_, reg_maps_, stream_);
+                                              (const float*)J_, (const float*)DF_, blocks_.data(), (int)blocks_.size());
+                launch_volume_reg3d(va, blocks_[b], (int)b, sa, status_, reg_maps_, stream_);
             }
             else if (vk == 1 && L_.ndim == 3)
                 launch_volume_fast3d(va, blocks_[b], sa, stream_);

@@ -438,9 +438,11 @@ __global__ void __launch_bounds__(NT, 2) k_fast3d(VolumeArgs<float> a, BlockDev 
 // (whose kernel finishes the node) perform the RK update.  blockIdx.z is the
 // face; threadIdx.x runs along the face's k extent (its j extent on the two
 // k faces), threadIdx.y along the other.  A node on several faces is handled
-// by its first face.
+// by its first face.  With kdone the marching kernel has already added the
+// k-face SATs and finished the nodes that lie on k faces only: the grid then
+// covers the x and y faces, and k-face SATs are not added again.
 template <bool PLASTIC>
-__global__ void __launch_bounds__(128) k_faces3d(VolumeArgs<float> a, BlockDev B, StageArgs sa) {
+__global__ void __launch_bounds__(128) k_faces3d(VolumeArgs<float> a, BlockDev B, StageArgs sa, int kdone) {
     const int fc = blockIdx.z, d = fc >> 1;
     const int n0 = B.n[0], n1 = B.n[1], n2 = B.n[2];
     const int nb = (d == 2) ? n1 : n2;
@@ -479,7 +481,7 @@ __global__ void __launch_bounds__(128) k_faces3d(VolumeArgs<float> a, BlockDev B
     for (int f2 = 0; f2 < 6; f2++) {
         if (!on[f2]) continue;
         if (B.defer[f2]) defer = true;
-        if (!B.bactive[f2]) continue;
+        if (!B.bactive[f2] || (kdone && f2 >= 4)) continue;
         const int fa = (f2 < 2) ? j : i;
         const int fb = (f2 >= 4) ? j : k;
         boundary_sat<float, 3, 2>(B, f2, fa, fb, (float)sa.dt, f, df, false);
@@ -540,7 +542,7 @@ void launch_order(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs
     dim3 grid(tk, tj, chunks);
     k_fast3d<ORDER><<<grid, NT, C::SMEM, s>>>(a, b, sa, chunk);
     const int nbmax = b.n[2] > b.n[1] ? b.n[2] : b.n[1], namax = b.n[0] > b.n[1] ? b.n[0] : b.n[1];
-    k_faces3d<PLASTIC><<<dim3((nbmax + 31) / 32, (namax + 3) / 4, 6), dim3(32, 4), 0, s>>>(a, b, sa);
+    k_faces3d<PLASTIC><<<dim3((nbmax + 31) / 32, (namax + 3) / 4, 6), dim3(32, 4), 0, s>>>(a, b, sa, 0);
     if (PLASTIC && sa.last) {
         const long long nin = (long long)(b.n[0] - 2) * (b.n[1] - 2) * (b.n[2] - 2);
         k_return_map3<<<(unsigned)((nin + 255) / 256), 256, 0, s>>>(a, b, sa);
@@ -567,9 +569,10 @@ bool fast3d_supported(const Layout& L, const BlockDev& b, int order) {
     return true;
 }
 
-void launch_faces3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s) {
+void launch_faces3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, bool kdone, cudaStream_t s) {
     const int nbmax = b.n[2] > b.n[1] ? b.n[2] : b.n[1], namax = b.n[0] > b.n[1] ? b.n[0] : b.n[1];
-    k_faces3d<false><<<dim3((nbmax + 31) / 32, (namax + 3) / 4, 6), dim3(32, 4), 0, s>>>(a, b, sa);
+    k_faces3d<false><<<dim3((nbmax + 31) / 32, (namax + 3) / 4, kdone ? 4 : 6), dim3(32, 4), 0, s>>>(a, b, sa,
+                                                                                                   kdone ? 1 : 0);
 }
 
 void launch_volume_fast3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s) {

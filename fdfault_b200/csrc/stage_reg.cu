@@ -22,8 +22,12 @@
 //  * interior stencils are unrolled in the antisymmetric form with immediate
 //    coefficients; y closure rows (whole warps) use the tabulated rows and
 //    the two k-edge tiles use one tap row per lane, as in stage_fast.cu;
-//  * nodes on a block face are written without the outer SAT and finished by
-//    the face-node kernel of stage_fast.cu.
+//  * outer SATs: a pre-pass (k_ksat3d, one thread per k-face node) evaluates
+//    the SAT increments of the two k faces from the stage-start fields into a
+//    compact per-block buffer; the k-edge tiles stage their rows of it with
+//    the plane and finish k-face nodes themselves, so their stores stay whole
+//    rows; nodes on x or y faces are written without those faces' SATs and
+//    finished by the face-node kernel of stage_fast.cu (coalesced along k).
 // Each staged box is one tensor copy over a (k, j, i, component) map whose k
 // origin is the 16-byte boundary at or below the tile's first column.  Every
 // mbarrier wait is bounded: on expiry the CTA records FDF_ERR_TIMEOUT, waits
@@ -34,6 +38,8 @@
 #include <atomic>
 #include <cstdint>
 #include <stdexcept>
+#include <string>
+#include <vector>
 
 #include "kernels.hpp"
 #include "sbp_coeffs.cuh"
@@ -51,6 +57,14 @@ struct RegMaps {
 struct RegMapsHost {
     RegMaps m;
     const float* F0;
+    // per block: k-face SAT increments [side][c][i][jp] and their tensor map
+    std::vector<float*> ksat;
+    std::vector<int> jp;
+    std::vector<CUtensorMap> kmap;
+    ~RegMapsHost() {
+        for (float* p : ksat)
+            if (p) cudaFree(p);
+    }
 };
 
 namespace {
@@ -59,6 +73,7 @@ constexpr int TJ = 8, TK = 32, NT = TJ * TK;
 constexpr int SW = TK + 4;   // staged row: 16-byte boundary at or below the tile's first column, 36 floats
 
 constexpr int up32(int n) { return (n + 31) / 32 * 32; }   // every box on a 128-byte boundary
+constexpr int KBJ = TJ + 4;   // staged k-face row: 16-byte boundary at or below the tile's first j
 
 template <int ORDER>
 struct RgCfg {
@@ -66,10 +81,12 @@ struct RgCfg {
     static constexpr int VH = TJ + 2 * H, VW = TK + 2 * H;
     static constexpr int BOX = TJ * SW;   // floats of one staged component
     // stage layout, floats: centre F[9], M[9], J, DF[9]; leading F[9], Mx[3], J
+    // k-edge tiles also stage their rows of the k-face SAT increments: per
+    // face side one box of KBJ j x 9 components
     static constexpr int CF = 0, CM = CF + up32(9 * BOX), CJ = CM + up32(9 * BOX), CD = CJ + up32(BOX),
                          LF = CD + up32(9 * BOX), LM = LF + up32(9 * BOX), LJ = LM + up32(3 * BOX),
-                         SSZ = LJ + up32(BOX);
-    static constexpr uint32_t BYTES = 4u * 41 * BOX;
+                         KSW = up32(9 * KBJ), KS = LJ + up32(BOX), SSZ = KS + 2 * KSW;
+    static constexpr uint32_t BYTES = 4u * 41 * BOX, KBYTES = 4u * 9 * KBJ;
     static constexpr int TY = 3 * VH * TK, TZ = 3 * TJ * VW;   // float2
     static constexpr int WROWS = 2 * NB + 1;
     static constexpr int WTAB = ((WROWS * NTB + 3) / 4) * 4;
@@ -96,7 +113,7 @@ struct HaloNode {
 template <int ORDER>
 __global__ void __launch_bounds__(NT, 2)
     k_reg3d(VolumeArgs<float> a, BlockDev B, StageArgs sa, int chunk, int* status,
-            const __grid_constant__ RegMaps maps, int fsel) {
+            const __grid_constant__ RegMaps maps, int fsel, const __grid_constant__ CUtensorMap kmap) {
     using C = RgCfg<ORDER>;
     constexpr int H = C::H, NB = C::NB, NTB = C::NTB, W = C::W, VH = C::VH, VW = C::VW, BOX = C::BOX;
     extern __shared__ __align__(128) float smem[];
@@ -134,6 +151,10 @@ __global__ void __launch_bounds__(NT, 2)
     const uint32_t bar0 = saddr(bars), bar1 = saddr(bars + 1);
 
     const bool kedge = (blockIdx.x == 0) || lastk;
+    // k faces whose SAT increments this tile stages (outer faces with a SAT)
+    const bool kf0 = (blockIdx.x == 0) && B.bactive[4], kf1 = lastk && B.bactive[5];
+    const int kjb = j0 & ~3;   // k-face box origin in j (block coordinates)
+    const uint32_t bytes = C::BYTES + (kf0 ? C::KBYTES : 0u) + (kf1 ? C::KBYTES : 0u);
     if (tid == 0) {
         bar_init(bar0);
         bar_init(bar1);
@@ -158,7 +179,7 @@ __global__ void __launch_bounds__(NT, 2)
         const uint32_t bar = b ? bar1 : bar0;
         const int ig = B.lo[0] + i;
         fence_proxy_async();
-        bar_expect(bar, C::BYTES);
+        bar_expect(bar, bytes);
         tma4(saddr(st + C::CF), mF, kgb, jg, ig, 0, bar);
         tma4(saddr(st + C::CM), &maps.M9, kgb, jg, ig, 0, bar);
         tma3(saddr(st + C::CJ), &maps.J, kgb, jg, ig, bar);
@@ -166,6 +187,8 @@ __global__ void __launch_bounds__(NT, 2)
         tma4(saddr(st + C::LF), mF, kgb, jg, ig + H, 0, bar);
         tma4(saddr(st + C::LM), &maps.M3, kgb, jg, ig + H, 0, bar);
         tma3(saddr(st + C::LJ), &maps.J, kgb, jg, ig + H, bar);
+        if (kf0) tma3(saddr(st + C::KS), &kmap, kjb, i, 0, bar);
+        if (kf1) tma3(saddr(st + C::KS + C::KSW), &kmap, kjb, i, 9, bar);
     };
     if (tid == 0) {
         issue(ib, 0);
@@ -245,7 +268,13 @@ __global__ void __launch_bounds__(NT, 2)
     const float lamc = (float)B.lam, gc = (float)B.g, g2c = (float)(2. * B.g);
     const float Acoef = (float)sa.A, Bcoef = (float)sa.B;
     const bool jint = (j >= NB) && (j < n1 - NB);
-    const bool face = (j == 0) | (j == n1 - 1) | (k == 0) | (k == n2 - 1);
+    const bool facexy = (j == 0) | (j == n1 - 1);   // (x faces: planes 0 and n0-1)
+    // this node's k face: 0 none, 1 SAT increment staged, 2 interface (finished there)
+    int kface = 0, kside = 0;
+    if (k == 0 || k == n2 - 1) {
+        kside = (k == 0) ? 0 : 1;
+        kface = B.defer[4 + kside] ? 2 : (B.bactive[4 + kside] ? 1 : 0);
+    }
 
     // x window: after the insert at plane i, wF/wv[m] hold plane i - H + m.
     // A chunk that starts past the left closure rows fills planes ib-H..ib+H-1
@@ -469,17 +498,46 @@ __global__ void __launch_bounds__(NT, 2)
             df[7] = fmaf(Acoef, df[7], gc * (e[1][2] + e[2][1]));
             df[8] = fmaf(Acoef, df[8], fmaf(g2c, e[2][2], lt));
         }
+        if (kface == 1) {   // k-face SAT increment staged by the pre-pass
+            const float* ks = st + C::KS + kside * C::KSW + (j - kjb);
+#pragma unroll
+            for (int c = 0; c < 9; c++) df[c] += ks[c * KBJ];
+        }
         if (owner) {
             const int id = colbase + i * s0;
 #pragma unroll
             for (int c = 0; c < 9; c++) DFg[c * cs + id] = df[c];
-            // face nodes: k_faces3d adds the outer SATs and finishes them
-            if (!(face | (i == 0) | (i == n0 - 1))) {
+            // x/y face nodes: k_faces3d adds those SATs and finishes them
+            if (!(facexy | (i == 0) | (i == n0 - 1) | (kface == 2))) {
 #pragma unroll
                 for (int c = 0; c < 9; c++) Fn[c * cs + id] = fmaf(Bcoef, df[c], st[C::CF + c * BOX + so]);
             }
         }
     }
+}
+
+// SAT increments of the two k faces of a block from the stage-start fields:
+// ks[side][c][i][jp] = the change the face's SAT makes to the rate of node
+// (i, j, k = 0 or n2-1).  One thread per face node, threads along j.
+__global__ void __launch_bounds__(128) k_ksat3d(VolumeArgs<float> a, BlockDev B, StageArgs sa, float* ks, int jp) {
+    const int side = blockIdx.z;
+    if (!B.bactive[4 + side]) return;
+    const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 4 + threadIdx.y;
+    const int n0 = B.n[0], n1 = B.n[1];
+    if (j >= n1 || i >= n0) return;
+    const int k = side ? B.n[2] - 1 : 0;
+    const long long cs = a.L.cstride;
+    const long long id = node_index(a.L, B.lo[0] + i, B.lo[1] + j, B.lo[2] + k);
+    float f[9], d[9];
+#pragma unroll
+    for (int c = 0; c < 9; c++) {
+        f[c] = a.F[c * cs + id];
+        d[c] = 0.f;
+    }
+    boundary_sat<float, 3, 2>(B, 4 + side, i, j, (float)sa.dt, f, d, false);
+    float* o = ks + (long long)side * 9 * n0 * jp + (long long)i * jp + j;
+#pragma unroll
+    for (int c = 0; c < 9; c++) o[(long long)c * n0 * jp] = d[c];
 }
 
 // choose the x chunk: the grid of tiles x chunks runs in whole waves of
@@ -501,7 +559,7 @@ int pick_chunk(int n0, int tiles, int slots, int H) {
 }
 
 template <int ORDER>
-void launch_order(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, int* status,
+void launch_order(const VolumeArgs<float>& a, const BlockDev& b, int bi, const StageArgs& sa, int* status,
                   const RegMapsHost& mh, cudaStream_t s) {
     using C = RgCfg<ORDER>;
     int dev = 0, nsm = 148;
@@ -523,14 +581,17 @@ void launch_order(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs
     const int chunks = (b.n[0] + chunk - 1) / chunk;
     dim3 grid(tk, tj, chunks);
     const int fsel = (a.F == mh.F0) ? 0 : 1;
-    k_reg3d<ORDER><<<grid, NT, C::SMEM, s>>>(a, b, sa, chunk, status, mh.m, fsel);
-    launch_faces3d(a, b, sa, s);
+    if (b.bactive[4] || b.bactive[5])
+        k_ksat3d<<<dim3((b.n[1] + 31) / 32, (b.n[0] + 3) / 4, 2), dim3(32, 4), 0, s>>>(a, b, sa, mh.ksat[bi],
+                                                                                      mh.jp[bi]);
+    k_reg3d<ORDER><<<grid, NT, C::SMEM, s>>>(a, b, sa, chunk, status, mh.m, fsel, mh.kmap[bi]);
+    launch_faces3d(a, b, sa, true, s);
 }
 
 }  // namespace
 
 RegMapsHost* make_reg_maps(const Layout& L, const float* F0, const float* F1, const float* M, const float* J,
-                           const float* DF) {
+                           const float* DF, const BlockDev* blocks, int nblocks) {
     RegMapsHost* h = new RegMapsHost;
     h->F0 = F0;
     const cuuint64_t d4[4] = {(cuuint64_t)L.s1, (cuuint64_t)L.nx[1], (cuuint64_t)L.nx[0], 9};
@@ -544,6 +605,23 @@ RegMapsHost* make_reg_maps(const Layout& L, const float* F0, const float* F1, co
         tma_encode(&h->m.M3, M, 4, d4, s4, b3);
         tma_encode(&h->m.J, J, 3, d3, s4, b1);
         tma_encode(&h->m.DF, DF, 4, d4, s4, b9);
+        h->ksat.assign(nblocks, nullptr);
+        h->jp.assign(nblocks, 0);
+        h->kmap.resize(nblocks);
+        for (int b = 0; b < nblocks; b++) {
+            const int n0 = blocks[b].n[0], jp = (blocks[b].n[1] + 3) / 4 * 4;
+            h->jp[b] = jp;
+            const size_t bytes = sizeof(float) * 18 * (size_t)n0 * jp;
+            const cudaError_t e = cudaMalloc(&h->ksat[b], bytes);
+            if (e != cudaSuccess)
+                throw std::runtime_error(std::string("CUDA error in cudaMalloc (k-face SAT buffer): ") +
+                                         cudaGetErrorString(e));
+            cudaMemset(h->ksat[b], 0, bytes);
+            const cuuint64_t dk[3] = {(cuuint64_t)jp, (cuuint64_t)n0, 18};
+            const cuuint64_t sk[2] = {(cuuint64_t)jp * 4, (cuuint64_t)n0 * jp * 4};
+            const cuuint32_t bk[3] = {KBJ, 1, 9};
+            tma_encode(&h->kmap[b], h->ksat[b], 3, dk, sk, bk);
+        }
     } catch (...) {
         delete h;
         throw;
@@ -563,7 +641,7 @@ bool reg3d_supported(const Layout& L, const BlockDev& b, int order) {
     return true;
 }
 
-void launch_volume_reg3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, int* status,
+void launch_volume_reg3d(const VolumeArgs<float>& a, const BlockDev& b, int bi, const StageArgs& sa, int* status,
                          const RegMapsHost* maps, cudaStream_t s) {
     if (a.cdiss > 0. || sa.plastic) {   // dissipation / plasticity: the tiled kernel of stage_fast.cu
         launch_volume_fast3d(a, b, sa, s);
@@ -571,9 +649,9 @@ void launch_volume_reg3d(const VolumeArgs<float>& a, const BlockDev& b, const St
     }
     if (!maps) throw std::runtime_error("register-window kernel: tensor maps missing");
     switch (a.order) {
-        case 2: launch_order<2>(a, b, sa, status, *maps, s); break;
-        case 3: launch_order<3>(a, b, sa, status, *maps, s); break;
-        default: launch_order<4>(a, b, sa, status, *maps, s); break;
+        case 2: launch_order<2>(a, b, bi, sa, status, *maps, s); break;
+        case 3: launch_order<3>(a, b, bi, sa, status, *maps, s); break;
+        default: launch_order<4>(a, b, bi, sa, status, *maps, s); break;
     }
 }
 
