@@ -27,8 +27,21 @@ U, DU, V, SS, SN, UX, DUX, VX, SX, STATE, DSTATE, DSTATEDT, TFRONT = range(13)
 _lib = None
 
 
-def build(ref_src: Optional[str] = "/root/reference/src", quiet: bool = True) -> None:
-    """Compile the oracle port, and the reference binary when its sources exist."""
+def reference_dir() -> str:
+    """The fdfault reference checkout: $FDFAULT_REFERENCE, else the directory
+    ``reference`` beside this repository (it may not exist, e.g. on machines
+    that only run the tests against the committed fixtures)."""
+    env = os.environ.get("FDFAULT_REFERENCE")
+    if env:
+        return env
+    return os.path.normpath(os.path.join(HERE, os.pardir, os.pardir, "reference"))
+
+
+def build(ref_src: Optional[str] = None, quiet: bool = True) -> None:
+    """Compile the oracle port, and the reference binary when its sources
+    exist (ref_src: the reference's src directory, default under reference_dir())."""
+    if ref_src is None:
+        ref_src = os.path.join(reference_dir(), "src")
     out = subprocess.DEVNULL if quiet else None
     subprocess.check_call(["make", "-C", HERE, "port"], stdout=out)
     if ref_src and os.path.isdir(ref_src):

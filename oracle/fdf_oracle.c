@@ -10,7 +10,7 @@
  * operation order (left-to-right products, same parenthesisation, same
  * accumulation order per node), and this file is compiled without FP
  * contraction, so results are bit-identical to the reference compiled the
- * same way (tests/test_oracle_ref.py pins this against oracle/_ref).
+ * same way (tests/test_oracle_golden.py pins this against fixtures written by oracle/_ref).
  *
  * Scope: ndim 2 (mode II and mode III) and 3; sbporder 2, 3, 4; RK orders
  * 1-4; elastic and plastic material; outer boundaries none / absorbing /

@@ -7,7 +7,9 @@ import pytest
 
 from fdfault_b200 import problems as P
 
-REF_PY = "/root/reference/python"
+import oracle
+
+REF_PY = os.path.join(oracle.reference_dir(), "python")
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_PY), reason="reference Python module not present")
