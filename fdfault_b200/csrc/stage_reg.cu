@@ -110,6 +110,11 @@ struct HaloNode {
     float s[6], v[3], m[3], J;
 };
 
+// (flux, velocity) pairs go through the paired FP32 instructions of sm_100
+// (each lane rounds as the scalar instruction would)
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 fma2(float a, float2 x, float2 acc) { return __ffma2_rn(make_float2(a, a), x, acc); }
+
 template <int ORDER>
 __global__ void __launch_bounds__(NT, 2)
     k_reg3d(VolumeArgs<float> a, BlockDev B, StageArgs sa, int chunk, int* status,
@@ -276,17 +281,23 @@ __global__ void __launch_bounds__(NT, 2)
         kface = B.defer[4 + kside] ? 2 : (B.bactive[4 + kside] ? 1 : 0);
     }
 
-    // x window: after the insert at plane i, wF/wv[m] hold plane i - H + m.
-    // A chunk that starts past the left closure rows fills planes ib-H..ib+H-1
-    // from global memory; the first chunk builds its window from the inserts.
-    float wF[W][3], wv[W][3];
+    // x window: after the insert at plane i, w[m][c] holds the pair
+    // (F_x,c , v_c) of plane i - H + m.  A chunk that starts past the left
+    // closure rows fills planes ib-H..ib+H-1 from global memory; the first
+    // chunk builds its window from the inserts.
+    float2 w[W][3];
 #pragma unroll
     for (int m = 0; m < W; m++)
 #pragma unroll
-        for (int c = 0; c < 3; c++) wF[m][c] = wv[m][c] = 0.f;
+        for (int c = 0; c < 3; c++) w[m][c] = make_float2(0.f, 0.f);
     if (ib >= NB && ib < n0 - NB) {
 #pragma unroll
-        for (int m = 1; m < W; m++) direct(ib - H - 1 + m, wF[m], wv[m]);
+        for (int m = 1; m < W; m++) {
+            float Fx[3], v[3];
+            direct(ib - H - 1 + m, Fx, v);
+#pragma unroll
+            for (int c = 0; c < 3; c++) w[m][c] = make_float2(Fx[c], v[c]);
+        }
     }
     HaloNode hn;
     load_halo(ib, hn);
@@ -307,15 +318,9 @@ __global__ void __launch_bounds__(NT, 2)
 #pragma unroll
             for (int m = 0; m < W - 1; m++)
 #pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    wF[m][c] = wF[m + 1][c];
-                    wv[m][c] = wv[m + 1][c];
-                }
+                for (int c = 0; c < 3; c++) w[m][c] = w[m + 1][c];
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                wF[W - 1][c] = Fx[c];
-                wv[W - 1][c] = v[c];
-            }
+            for (int c = 0; c < 3; c++) w[W - 1][c] = make_float2(Fx[c], v[c]);
         }
         // ---- centre plane i: y/z flux tiles of the tile and of this thread's halo node
         {
@@ -358,40 +363,30 @@ __global__ void __launch_bounds__(NT, 2)
             issued++;
         }
 
-        // ---- derivatives: DFl[d][c] of the fluxes, Dv[d][c] of the velocities
-        float DFl[3][3], Dv[3][3];
+        // ---- derivatives: D[d][c] = (d/dxi_d of the flux F_d,c , of the velocity v_c)
+        float2 D[3][3];
         if (i >= NB && i < n0 - NB) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                float af = 0.f, av = 0.f;
+                float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
-                for (int n = 1; n <= H; n++) {
-                    af = fmaf(inner_c<ORDER>(n), wF[H + n][c] - wF[H - n][c], af);
-                    av = fmaf(inner_c<ORDER>(n), wv[H + n][c] - wv[H - n][c], av);
-                }
-                DFl[0][c] = af;
-                Dv[0][c] = av;
+                for (int n = 1; n <= H; n++) acc = fma2(inner_c<ORDER>(n), sub2(w[H + n][c], w[H - n][c]), acc);
+                D[0][c] = acc;
             }
         } else {   // x closure rows: 3H taps from global memory
             const bool left = i < NB;
             const int row = left ? i + 1 : n0 - i;
             const float sg = left ? 1.f : -1.f;
-            float af[3] = {0.f, 0.f, 0.f}, av[3] = {0.f, 0.f, 0.f};
+            float2 acc[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
             for (int n = 0; n < NTB; n++) {
                 const float cf = sbp_coef<float>(ORDER, row, n);
                 float Fx[3], v[3];
                 direct(left ? n : n0 - 1 - n, Fx, v);
 #pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    af[c] = fmaf(cf, Fx[c], af[c]);
-                    av[c] = fmaf(cf, v[c], av[c]);
-                }
+                for (int c = 0; c < 3; c++) acc[c] = fma2(cf, make_float2(Fx[c], v[c]), acc[c]);
             }
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                DFl[0][c] = sg * af[c];
-                Dv[0][c] = sg * av[c];
-            }
+            for (int c = 0; c < 3; c++) D[0][c] = __fmul2_rn(make_float2(sg, sg), acc[c]);
         }
         // closure rows this tile does not write may have taps outside the tile:
         // they take the interior form (taps in the tile and its halo), discarded
@@ -399,16 +394,12 @@ __global__ void __launch_bounds__(NT, 2)
         if (jint || jskip) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                float af = 0.f, av = 0.f;
+                float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
-                for (int n = 1; n <= H; n++) {
-                    const float2 p = ty[(c * VH + tj + H + n) * TK + tk];
-                    const float2 q = ty[(c * VH + tj + H - n) * TK + tk];
-                    af = fmaf(inner_c<ORDER>(n), p.x - q.x, af);
-                    av = fmaf(inner_c<ORDER>(n), p.y - q.y, av);
-                }
-                DFl[1][c] = af;
-                Dv[1][c] = av;
+                for (int n = 1; n <= H; n++)
+                    acc = fma2(inner_c<ORDER>(n),
+                               sub2(ty[(c * VH + tj + H + n) * TK + tk], ty[(c * VH + tj + H - n) * TK + tk]), acc);
+                D[1][c] = acc;
             }
         } else {
             const bool left = j < NB;
@@ -417,51 +408,43 @@ __global__ void __launch_bounds__(NT, 2)
             const float sg = left ? 1.f : -1.f;
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                float af = 0.f, av = 0.f;
-                for (int n = 0; n < NTB; n++) {
-                    const float cf = sbp_coef<float>(ORDER, row, n);
-                    const float2 p = ty[(c * VH + base + n * step) * TK + tk];
-                    af = fmaf(cf, p.x, af);
-                    av = fmaf(cf, p.y, av);
-                }
-                DFl[1][c] = sg * af;
-                Dv[1][c] = sg * av;
+                float2 acc = make_float2(0.f, 0.f);
+                for (int n = 0; n < NTB; n++)
+                    acc = fma2(sbp_coef<float>(ORDER, row, n), ty[(c * VH + base + n * step) * TK + tk], acc);
+                D[1][c] = __fmul2_rn(make_float2(sg, sg), acc);
             }
         }
         if (!kedge) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                float af = 0.f, av = 0.f;
+                float2 acc = make_float2(0.f, 0.f);
 #pragma unroll
-                for (int n = 1; n <= H; n++) {
-                    const float2 p = tz[(c * TJ + tj) * VW + tk + H + n];
-                    const float2 q = tz[(c * TJ + tj) * VW + tk + H - n];
-                    af = fmaf(inner_c<ORDER>(n), p.x - q.x, af);
-                    av = fmaf(inner_c<ORDER>(n), p.y - q.y, av);
-                }
-                DFl[2][c] = af;
-                Dv[2][c] = av;
+                for (int n = 1; n <= H; n++)
+                    acc = fma2(inner_c<ORDER>(n),
+                               sub2(tz[(c * TJ + tj) * VW + tk + H + n], tz[(c * TJ + tj) * VW + tk + H - n]), acc);
+                D[2][c] = acc;
             }
         } else {
-            float af[3] = {0.f, 0.f, 0.f}, av[3] = {0.f, 0.f, 0.f};
+            float2 acc[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
             const float2* trow = tz + tj * VW;
 #pragma unroll
             for (int n = 0; n < NTB; n++) {
-                const float w = wtab[kw + n];
+                const float wt = wtab[kw + n];
                 const int col = kb + ks * min(n, kmax);
 #pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    const float2 p = trow[c * TJ * VW + col];
-                    af[c] = fmaf(w, p.x, af[c]);
-                    av[c] = fmaf(w, p.y, av[c]);
-                }
+                for (int c = 0; c < 3; c++) acc[c] = fma2(wt, trow[c * TJ * VW + col], acc[c]);
             }
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                DFl[2][c] = af[c];
-                Dv[2][c] = av[c];
-            }
+            for (int c = 0; c < 3; c++) D[2][c] = acc[c];
         }
+        float DFl[3][3], Dv[3][3];
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                DFl[d][c] = D[d][c].x;
+                Dv[d][c] = D[d][c].y;
+            }
         __syncthreads();   // flux tiles are rewritten for the next plane
 
         // ---- rate: df = A df + L(f), then the RK update
