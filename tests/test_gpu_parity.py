@@ -4,7 +4,8 @@ The FP64 path replays the reference's operation order, so every output unit
 value and rupture time must be identical to the reference solver's output
 (golden fixtures).  Exceptions: the STZ friction law evaluates exp/log inside
 the per-stage Newton solve, where CUDA's and glibc's last bits can differ; for
-those cases the tolerance is relative L2 <= 1e-9 per output unit.
+those cases the tolerance is the FP64 contract, relative L2 <= 1e-10 per output
+unit (the measured value is printed).
 """
 
 import os
@@ -56,7 +57,9 @@ def test_fp64_matches_reference(name, tmp_path):
         a, b = got[key], ref
         assert a.shape == b.shape, key
         if name in cases.LIBM_CASES and not key.startswith("t/"):
-            assert rel_l2(a, b) <= 1e-9, (key, rel_l2(a, b))
+            # measured values are printed; the bound is the FP64 contract
+            print(name, key, "relative L2 %.3g" % rel_l2(a, b))
+            assert rel_l2(a, b) <= 1e-10, (key, rel_l2(a, b))
         else:
             assert np.array_equal(a, b), "%s max diff %g" % (key, np.max(np.abs(a - b)))
 
