@@ -84,7 +84,7 @@ def wait_bounded(proc, timeout=REF_TIMEOUT_S):
 def build_problem(workdir, nt, **size):
     from fdfault_b200 import problems as P
 
-    prob = P.planar3d(nt=nt, name="planar3d", datadir=workdir + "/", workdir=workdir, seed=1234,
+    prob = P.planar3d(nt=nt, name="planar3d", datadir=workdir + "/", workdir=workdir, seed=1234, cfl=P.WORKLOAD_CFL_3D,
                       nx=size["nx"], ny=size["ny"], nz=size["nz"], h=size["h"])
     return prob.write(os.path.join(workdir, "planar3d.in")), prob
 
@@ -253,7 +253,8 @@ def run_stz(args, local):
     ncollect, epochs = 24, 20
     nrun = args.warmup + args.steps + 2
     tmp = tempfile.mkdtemp(prefix="fdf_stz_")
-    prob = P.stz3d(nt=max(ncollect, nrun) + 2, name="stz3d", datadir=tmp + "/", workdir=tmp, **size)
+    prob = P.stz3d(nt=max(ncollect, nrun) + 2, name="stz3d", datadir=tmp + "/", workdir=tmp, cfl=P.WORKLOAD_CFL_3D,
+                   **size)
     infile = prob.write(os.path.join(tmp, "stz3d.in"))
     with fs.Problem(infile, precision=fs.FP32, device=local) as p:
         p.stz_collect(2_400_000)
@@ -513,7 +514,8 @@ def run_rough(args, local):
     size = dict(nx=601, ny=301, nz=301, h=0.1) if args.size == "full" else dict(nx=201, ny=101, nz=101, h=0.3)
     tmp = tempfile.mkdtemp(prefix="fdf_rough_")
     t0 = time.perf_counter()
-    prob = P.rough3d(nt=args.warmup + args.steps + 8, name="rough3d", datadir=tmp + "/", workdir=tmp, **size)
+    prob = P.rough3d(nt=args.warmup + args.steps + 8, name="rough3d", datadir=tmp + "/", workdir=tmp,
+                     cfl=P.WORKLOAD_CFL_3D, **size)
     infile = prob.write(os.path.join(tmp, "rough3d.in"))
     gen_s = time.perf_counter() - t0
     t0 = time.perf_counter()

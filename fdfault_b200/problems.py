@@ -265,6 +265,14 @@ def lognormal_field(n0: int, n1: int, h: float, mean: float, sd: float, corr: fl
     return np.exp(mu_ln + np.sqrt(s2) * g)
 
 
+# CFL number of the full-size 3D workloads (two blocks of 401 x 201 x 201 at
+# h = 0.1 km, RK3).  At CFL 0.3 and 0.25 both precisions grow without bound at
+# the corners where the fault meets the absorbing x and z- faces after about
+# 180 and 450 steps (the SAT terms of three faces stack there and RK3's
+# stability interval is exceeded); at 0.2 and 0.15 1500 steps stay bounded.
+WORKLOAD_CFL_3D = 0.2
+
+
 def planar3d(nx: int = 401, ny: int = 201, nz: int = 201, h: float = 0.1, nt: int = 1500,
              name: str = "planar3d", datadir: str = "data/", workdir: str = ".", seed: int = 1234,
              rkorder: int = 3, sbporder: int = 4, cfl: float = 0.3, mus_mean: float = 0.677,

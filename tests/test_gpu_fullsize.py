@@ -84,7 +84,7 @@ def test_planar3d_full_size_fp32_against_fp64(tmp_path):
     tmp = str(tmp_path)
     nsteps = 300
     prob = P.planar3d(nt=nsteps + 2, name="planar3d", datadir=tmp + "/", workdir=tmp, seed=1234,
-                      nx=401, ny=201, nz=201, h=0.1)
+                      nx=401, ny=201, nz=201, h=0.1, cfl=P.WORKLOAD_CFL_3D)
     infile = prob.write(os.path.join(tmp, "planar3d.in"))
     keys = (fs.U, fs.V, fs.S)
 
