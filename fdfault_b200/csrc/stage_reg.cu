@@ -91,7 +91,7 @@ struct RgCfg {
     static constexpr int WROWS = 2 * NB + 1;
     static constexpr int WTAB = ((WROWS * NTB + 3) / 4) * 4;
     static constexpr size_t SMEM =
-        sizeof(float) * 2 * SSZ + sizeof(float2) * (TY + TZ) + sizeof(float) * WTAB + 2 * sizeof(uint64_t);
+        sizeof(float) * 2 * SSZ + sizeof(float2) * (TY + TZ) + sizeof(float) * WTAB + 6 * sizeof(uint64_t);
 };
 
 template <int ORDER>
@@ -154,6 +154,12 @@ __global__ void __launch_bounds__(NT, 2)
     const int jg = B.lo[1] + j0;
     const CUtensorMap* mF = &maps.F[fsel];
     const uint32_t bar0 = saddr(bars), bar1 = saddr(bars + 1);
+    // warp-arrival barriers of the march (one arrival per warp and plane):
+    // flux tiles written, flux tiles read, stage consumed
+    constexpr uint32_t NWARP = NT / 32;
+    const uint32_t barT = saddr(bars + 2), barR = saddr(bars + 3), barS = saddr(bars + 4);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 5);
+    const int lane = tid & 31;
 
     const bool kedge = (blockIdx.x == 0) || lastk;
     // k faces whose SAT increments this tile stages (outer faces with a SAT)
@@ -163,6 +169,10 @@ __global__ void __launch_bounds__(NT, 2)
     if (tid == 0) {
         bar_init(bar0);
         bar_init(bar1);
+        bar_init_count(barT, NWARP);
+        bar_init_count(barR, NWARP);
+        bar_init_count(barS, NWARP);
+        *abort_flag = 0;
         bar_init_fence();
     }
     if (kedge && tid < C::WROWS * NTB) {
@@ -304,9 +314,22 @@ __global__ void __launch_bounds__(NT, 2)
 
     const int so = tj * SW + tk + kofs;   // this node in a staged component
     for (int i = ib; i < ie; i++) {
-        const int b = (i - ib) & 1;
+        const int kk = i - ib;
+        const int b = kk & 1;
         const float* st = stg + b * C::SSZ;
-        const bool ok = bar_wait(b ? bar1 : bar0, ((i - ib) >> 1) & 1, wlim);
+        if (kk > 0) {
+            // every warp has read plane i-1's flux tiles (they are rewritten below);
+            // once every warp is also done with plane i-1's stage, plane i+1 goes into it
+            if (!bar_wait(barR, (kk - 1) & 1, TMA_DRAIN_LIMIT)) *abort_flag = 1;
+            if (tid == 0 && issued < ie) {
+                if (bar_wait(barS, (kk - 1) & 1, TMA_DRAIN_LIMIT))
+                    issue(issued, (issued - ib) & 1);
+                else
+                    *abort_flag = 1;
+            }
+            if (issued < ie) issued++;
+        }
+        if (!bar_wait(b ? bar1 : bar0, (kk >> 1) & 1, wlim)) *abort_flag = 1;
         // ---- leading plane i+H enters the x window
         if (i + H < n0) {
             float s[6], v[3], Fx[3];
@@ -349,19 +372,8 @@ __global__ void __launch_bounds__(NT, 2)
             }
         }
         if (i + 1 < ie) load_halo(i + 1, hn);
-        if (__syncthreads_or(!ok)) {   // flux tiles ready; every thread is done with plane i-1's stage
-            if (tid == 0) {
-                atomicOr(status, FDF_ERR_TIMEOUT);
-                // wait for the copies still in flight before the CTA leaves
-                for (int q = i; q < issued; q++)
-                    bar_wait((q - ib) & 1 ? bar1 : bar0, ((q - ib) >> 1) & 1, TMA_DRAIN_LIMIT);
-            }
-            return;
-        }
-        if (i > ib && issued < ie) {   // plane i+1 into the stage plane i-1 used
-            if (tid == 0) issue(issued, (issued - ib) & 1);
-            issued++;
-        }
+        __syncwarp();
+        if (lane == 0) bar_arrive(barT);
 
         // ---- derivatives: D[d][c] = (d/dxi_d of the flux F_d,c , of the velocity v_c)
         float2 D[3][3];
@@ -387,6 +399,16 @@ __global__ void __launch_bounds__(NT, 2)
             }
 #pragma unroll
             for (int c = 0; c < 3; c++) D[0][c] = __fmul2_rn(make_float2(sg, sg), acc[c]);
+        }
+        // flux tiles of plane i complete; a wait that ran out anywhere ends the CTA
+        if (!bar_wait(barT, kk & 1, TMA_DRAIN_LIMIT) || *abort_flag) {
+            if (tid == 0) {
+                atomicOr(status, FDF_ERR_TIMEOUT);
+                // wait for the copies still in flight before the CTA leaves
+                for (int q = i; q < issued; q++)
+                    bar_wait((q - ib) & 1 ? bar1 : bar0, ((q - ib) >> 1) & 1, TMA_DRAIN_LIMIT);
+            }
+            return;
         }
         // closure rows this tile does not write may have taps outside the tile:
         // they take the interior form (taps in the tile and its halo), discarded
@@ -445,7 +467,8 @@ __global__ void __launch_bounds__(NT, 2)
                 DFl[d][c] = D[d][c].x;
                 Dv[d][c] = D[d][c].y;
             }
-        __syncthreads();   // flux tiles are rewritten for the next plane
+        __syncwarp();
+        if (lane == 0) bar_arrive(barR);   // this warp is done with the flux tiles
 
         // ---- rate: df = A df + L(f), then the RK update
         float df[9];
@@ -496,6 +519,8 @@ __global__ void __launch_bounds__(NT, 2)
                 for (int c = 0; c < 9; c++) Fn[c * cs + id] = fmaf(Bcoef, df[c], st[C::CF + c * BOX + so]);
             }
         }
+        __syncwarp();
+        if (lane == 0) bar_arrive(barS);   // this warp is done with the stage of plane i
     }
 }
 

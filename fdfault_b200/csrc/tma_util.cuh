@@ -18,6 +18,13 @@ __device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cv
 __device__ __forceinline__ void bar_init(uint32_t bar) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(1) : "memory");
 }
+__device__ __forceinline__ void bar_init_count(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+// one arrival (release semantics at CTA scope)
+__device__ __forceinline__ void bar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
 __device__ __forceinline__ void bar_init_fence() {
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
