@@ -32,10 +32,12 @@ sys.path.insert(0, HERE)
 
 METRIC = "node-stage updates/s"
 WORKLOAD = dict(nx=401, ny=201, nz=201, h=0.1)
-# reduced instance of the same problem for ncu captures (4.1M nodes, still far larger than L2)
-PROFILE_WORKLOAD = dict(nx=201, ny=101, nz=101, h=0.2)
+# reduced instance of the same problem for ncu captures: the full-size cross-section
+# (the same 26 x 7 tiles per plane) over half the planes; 16.2M nodes, 2.4 GB
+PROFILE_WORKLOAD = dict(nx=201, ny=201, nz=201, h=0.1)
 CPU_SAMPLE = dict(nx=101, ny=51, nz=51, h=0.4)
-PROFILE_TRAFFIC = os.path.join(HERE, "profiles", "volume_fast3d_planar3d.md")
+PROFILE_TRAFFIC = {1: os.path.join(HERE, "profiles", "volume_fast3d_planar3d.md"),
+                   3: os.path.join(HERE, "profiles", "volume_regwindow3d_planar3d.md")}
 KERNEL_NAMES = {0: "volume_exact", 1: "volume_tiled3d", 2: "volume_staged3d", 3: "volume_regwindow3d"}
 
 
@@ -55,9 +57,9 @@ def parse():
                          "rupture in FP64; ensemble: 256 2D ruptures of uneven sizes, batched; rough: "
                          "rough fault with plasticity, two blocks of 601x301x301, FP32")
     ap.add_argument("--members", type=int, default=256, help="ensemble members (all ranks together)")
-    ap.add_argument("--volume-kernel", type=int, default=1, choices=[0, 1, 2, 3],
-                    help="FP32 3D volume kernel: 0 reference order, 1 tiled (default), 2 staged (TMA), "
-                         "3 register window (TMA-staged planes)")
+    ap.add_argument("--volume-kernel", type=int, default=3, choices=[0, 1, 2, 3],
+                    help="FP32 3D volume kernel: 0 reference order, 1 tiled, 2 staged (TMA), "
+                         "3 register window (TMA-staged planes, default)")
     return ap.parse_args()
 
 
@@ -152,10 +154,10 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per node-stage of the volume kernel from the committed ncu summary, or None."""
+def profiled_traffic(kind):
+    """DRAM bytes per node-stage of volume kernel `kind` from its committed ncu summary, or None."""
     try:
-        with open(PROFILE_TRAFFIC) as fh:
+        with open(PROFILE_TRAFFIC[kind]) as fh:
             for line in fh:
                 if line.startswith("traffic_bytes_per_node_stage:"):
                     return float(line.split(":")[1].split()[0])
@@ -676,7 +678,7 @@ def main():
     vol_avg_ms = vol_ms / max(vol_n, 1)
     bytes_per_launch = bps * nodes / nblocks
     achieved = bytes_per_launch / (vol_avg_ms * 1e-3) / 1e9
-    traffic_pn = profiled_traffic()
+    traffic_pn = profiled_traffic(vk)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": peak_kind, "kernel": KERNEL_NAMES[vk],
                 "algorithmic_bytes_per_node_stage": bps,

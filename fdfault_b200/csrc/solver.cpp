@@ -773,8 +773,8 @@ void Solver::profile_read(int kernel, double* total_ms, long long* launches) {
 
 int Solver::volume_kernel_active() const {
     if (vkernel_ == 0 || precision_ != 1) return 0;
-    if (L_.ndim == 2) {   // tiled 2D kernel (elastic, no dissipation) or none
-        if (vkernel_ != 1 || P_.plastic() || P_.cdiss > 0.) return 0;
+    if (L_.ndim == 2) {   // tiled 2D kernel (elastic, no dissipation; kinds 1 and 3) or none
+        if ((vkernel_ != 1 && vkernel_ != 3) || P_.plastic() || P_.cdiss > 0.) return 0;
         for (auto& B : blocks_)
             if (!fast2d_supported(L_, B, P_.sbporder)) return 0;
         return 1;

@@ -134,7 +134,7 @@ class Solver {
     int nt_ = 0, nstages_ = 0;
     double A_[5] = {0}, B_[5] = {0}, C_[6] = {0};
     int step_index_ = 0;
-    int vkernel_ = 1;
+    int vkernel_ = 3;   // FP32 default: register-window 3D kernel (2D: the tiled 2D kernel)
     StagedMapsHost* staged_maps_ = nullptr;   // tensor maps of the FP32 arrays (staged kernel)
     RegMapsHost* reg_maps_ = nullptr;         // tensor maps of the FP32 arrays (register-window kernel)
     long long wait_limit_ = 1LL << 22;        // polls of a bounded mbarrier wait (TMA-staged kernels)

@@ -145,14 +145,14 @@ int fdf_use_graphs(fdf_handle* h, int on);
 int fdf_use_fast_kernel(fdf_handle* h, int on, int* active);
 
 /* FP32 volume kernel by kind: 0 one thread per node (reference operation
- * order), 1 tiled (the default: 3D blocks of at least 8 x 32 in y x z, and 2D
- * elastic blocks at least 32 nodes wide in y), 2 staged (3D only: planes
- * brought into shared memory by TMA tensor copies), 3 register window (3D
- * only, same block sizes as kind 1: the x stencil window in registers, every
- * plane of a tile staged by TMA tensor copies; plastic or dissipative stages
- * run kind 1).  active = the kind that
- * will run (0 where the chosen one does not apply to the problem; FP64
- * problems always run kind 0). */
+ * order), 1 tiled (3D blocks of at least 8 x 32 in y x z, and 2D elastic
+ * blocks at least 32 nodes wide in y), 2 staged (3D only: planes brought into
+ * shared memory by TMA tensor copies), 3 register window (the default: 3D
+ * blocks of the same sizes as kind 1, the x stencil window in registers and
+ * every plane of a tile staged by TMA tensor copies; plastic or dissipative
+ * stages run kind 1; for 2D problems it selects the tiled 2D kernel like
+ * kind 1).  active = the kind that will run (0 where the chosen one does not
+ * apply to the problem; FP64 problems always run kind 0). */
 int fdf_set_volume_kernel(fdf_handle* h, int kind, int* active);
 
 /* Polls of each bounded wait for staged data in the TMA-staged volume kernels
