@@ -330,21 +330,6 @@ __global__ void __launch_bounds__(NT, 2)
             if (issued < ie) issued++;
         }
         if (!bar_wait(b ? bar1 : bar0, (kk >> 1) & 1, wlim)) *abort_flag = 1;
-        // ---- leading plane i+H enters the x window
-        if (i + H < n0) {
-            float s[6], v[3], Fx[3];
-#pragma unroll
-            for (int c = 0; c < 6; c++) s[c] = st[C::LF + (3 + c) * BOX + so];
-#pragma unroll
-            for (int c = 0; c < 3; c++) v[c] = st[C::LF + c * BOX + so];
-            fluxes(st[C::LJ + so], st[C::LM + so], st[C::LM + BOX + so], st[C::LM + 2 * BOX + so], s, Fx);
-#pragma unroll
-            for (int m = 0; m < W - 1; m++)
-#pragma unroll
-                for (int c = 0; c < 3; c++) w[m][c] = w[m + 1][c];
-#pragma unroll
-            for (int c = 0; c < 3; c++) w[W - 1][c] = make_float2(Fx[c], v[c]);
-        }
         // ---- centre plane i: y/z flux tiles of the tile and of this thread's halo node
         {
             float s[6], Fy[3], Fz[3];
@@ -371,9 +356,26 @@ __global__ void __launch_bounds__(NT, 2)
                     tz[(c * TJ + hj) * VW + hk + H] = make_float2(Fh[c], hn.v[c]);
             }
         }
-        if (i + 1 < ie) load_halo(i + 1, hn);
         __syncwarp();
         if (lane == 0) bar_arrive(barT);
+        // work that the flux tiles do not wait for: the next halo node's loads
+        // and the leading plane's entry into the x window
+        if (i + 1 < ie) load_halo(i + 1, hn);
+        // ---- leading plane i+H enters the x window
+        if (i + H < n0) {
+            float s[6], v[3], Fx[3];
+#pragma unroll
+            for (int c = 0; c < 6; c++) s[c] = st[C::LF + (3 + c) * BOX + so];
+#pragma unroll
+            for (int c = 0; c < 3; c++) v[c] = st[C::LF + c * BOX + so];
+            fluxes(st[C::LJ + so], st[C::LM + so], st[C::LM + BOX + so], st[C::LM + 2 * BOX + so], s, Fx);
+#pragma unroll
+            for (int m = 0; m < W - 1; m++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) w[m][c] = w[m + 1][c];
+#pragma unroll
+            for (int c = 0; c < 3; c++) w[W - 1][c] = make_float2(Fx[c], v[c]);
+        }
 
         // ---- derivatives: D[d][c] = (d/dxi_d of the flux F_d,c , of the velocity v_c)
         float2 D[3][3];
