@@ -38,6 +38,7 @@ PROFILE_WORKLOAD = dict(nx=201, ny=201, nz=201, h=0.1)
 CPU_SAMPLE = dict(nx=101, ny=51, nz=51, h=0.4)
 PROFILE_TRAFFIC = {1: os.path.join(HERE, "profiles", "volume_fast3d_planar3d.md"),
                    3: os.path.join(HERE, "profiles", "volume_regwindow3d_planar3d.md")}
+PLANAR_WORKLOAD_NAME = "planar3d: 2 blocks 401x201x201, slip weakening, log-normal mus, RK3 at CFL 0.2"
 KERNEL_NAMES = {0: "volume_exact", 1: "volume_tiled3d", 2: "volume_staged3d", 3: "volume_regwindow3d"}
 
 
@@ -50,6 +51,9 @@ def parse():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the other workloads (FP64 planar, 2D FP64, STZ, ensemble, rough) that a full-size "
+                         "single-GPU run records under 'extras'")
     ap.add_argument("--size", default="full", choices=["full", "profile"],
                     help="profile: 2x201x101x101 instance for ncu captures")
     ap.add_argument("--config", default="planar", choices=["planar", "stz", "mode2", "ensemble", "rough"],
@@ -204,37 +208,67 @@ def cpu_reference_sample(workdir, nsteps, nproc):
     return total / max(secs), kind, nproc, max(secs)
 
 
-def cpu_workers():
-    """Host threads to use: all cores, bounded by memory (~0.5 GB per sample run)."""
+def cpu_workers(bytes_per_run=512 << 20):
+    """Host threads to use: all cores, bounded by memory (bytes_per_run per sample run)."""
     n = os.cpu_count() or 1
     try:
         mem = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES")
-        n = min(n, max(1, int(mem // (512 << 20))))
+        n = min(n, max(1, int(0.8 * mem // bytes_per_run)))
     except (ValueError, OSError):
         pass
     return max(1, min(n, 128))
 
 
+REF_FULL_BYTES = 10 << 30   # resident memory of one reference process on the full planar grid (9.0 GB measured)
+
+
 def run_reference_arm(args, rank, world):
+    """The reference solver on the host cores, on the same workload as the GPU
+    arm: the full planar grid (two blocks of 401x201x201, the identical .in
+    file), one process per core (bounded by memory), each timing one RK3 step
+    of its own copy; the value is all processes' node-stages over the slowest
+    process's time-stepping loop.  A full-grid step takes about a minute per
+    process, so the arm times one sample whatever --steps is."""
     if rank != 0:
         return
-    nproc = cpu_workers()
+    import oracle
+
+    nproc = cpu_workers(REF_FULL_BYTES)
     tmp = tempfile.mkdtemp(prefix="fdf_refarm_")
-    rates, secs = [], []
-    kind = None
-    for i in range(args.warmup + args.steps):
-        rate, kind, cores, s = cpu_reference_sample(os.path.join(tmp, "s%d" % i), 1, nproc)
-        if i >= args.warmup:
-            rates.append(rate)
-            secs.append(s)
-    value = float(np.mean(rates))
-    nodes = CPU_SAMPLE["nx"] * (2 * CPU_SAMPLE["ny"]) * CPU_SAMPLE["nz"]
-    sample = ("%d concurrent single-process runs of the same problem at 101x51x51 nodes per block, 1 RK3 step "
-              "each, per timed step; time-stepping loop only" % nproc)
+    nodes = WORKLOAD["nx"] * 2 * WORKLOAD["ny"] * WORKLOAD["nz"]
+    runs = []
+    for r in range(nproc):
+        d = os.path.join(tmp, "r%d" % r)
+        os.makedirs(d, exist_ok=True)
+        infile, _ = build_problem(d, 1, **WORKLOAD)
+        runs.append((d, infile))
+    if os.path.exists(oracle.REF_BIN):
+        kind = "reference"
+        procs = []
+        for d, infile in runs:
+            tf = os.path.join(d, "timing.txt")
+            procs.append((subprocess.Popen([oracle.REF_BIN, infile], cwd=d, env=dict(os.environ, FDF_REF_TIMING=tf),
+                                           stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL), tf))
+        secs = []
+        for pr, tf in procs:
+            wait_bounded(pr, timeout=900)
+            with open(tf) as fh:
+                secs.append(float(fh.read().split()[-1]))
+    else:
+        kind = "port"
+        code = ("import sys,time; sys.path.insert(0,%r); import oracle; o=oracle.Oracle(sys.argv[1]); "
+                "t=time.perf_counter(); o.run(1); print(time.perf_counter()-t)") % HERE
+        procs = [subprocess.Popen([sys.executable, "-c", code, infile], stdout=subprocess.PIPE, text=True)
+                 for _, infile in runs]
+        secs = [float(pr.communicate(timeout=900)[0].split()[-1]) for pr in procs]
+    value = nodes * 3 * nproc / max(secs)
+    sample = ("%d concurrent single-process runs of the full workload (2x401x201x201, the same input file), one "
+              "RK3 step each; time-stepping loop only (slowest %.1f s)" % (nproc, max(secs)))
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "node-stage/s", "n_gpus": args.gpus,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(secs)),
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * max(secs),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "planar3d 2x401x201x201 (sampled at 2x101x51x51)", "nodes_per_sample": nodes * nproc},
+           "config": {"workload": PLANAR_WORKLOAD_NAME, "nodes": nodes, "stages_per_step": 3,
+                      "timed_rk3_steps_per_process": 1, "processes": nproc},
            "cpu_baseline": {"value": value, "unit": "node-stage/s", "cores": nproc, "kind": kind, "sample": sample},
            "e2e": {"value": value, "unit": "node-stage/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
@@ -584,6 +618,39 @@ def run_rough(args, local):
     print(json.dumps(out), flush=True)
 
 
+EXTRAS = [
+    ("planar3d_fp64", ["--precision", "fp64", "--steps", "10", "--warmup", "3", "--e2e-steps", "20"]),
+    ("mode2_fp64", ["--config", "mode2", "--steps", "100", "--warmup", "10"]),
+    ("stz_learned", ["--config", "stz", "--steps", "10", "--warmup", "3"]),
+    ("ensemble_256", ["--config", "ensemble", "--steps", "20", "--warmup", "3"]),
+    ("rough_plastic", ["--config", "rough", "--steps", "6", "--warmup", "2"]),
+]
+EXTRA_KEYS = ("value", "unit", "ms_per_step", "dtype", "config", "roofline", "kernel_ms", "e2e", "plain", "learned",
+              "learned_vs_plain_rel_l2", "training", "one_problem_at_a_time", "judges")
+
+
+def run_extras():
+    """The other workloads, each as its own bench.py process (one GPU, bounded
+    time): their JSON lines, trimmed, keyed by workload; a failure is recorded
+    and does not stop the others."""
+    res = {}
+    for name, argv in EXTRAS:
+        cmd = [sys.executable, os.path.join(HERE, "bench.py"), "--no-cpu-baseline", "--no-extras"] + argv
+        t0 = time.perf_counter()
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+            lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+            if r.returncode != 0 or not lines:
+                res[name] = {"error": "rc %d: %s" % (r.returncode, (r.stderr or r.stdout).strip()[-300:])}
+                continue
+            d = json.loads(lines[-1])
+            res[name] = {k: d[k] for k in EXTRA_KEYS if k in d}
+        except Exception as e:   # noqa: BLE001 - recorded, the headline stands
+            res[name] = {"error": repr(e)[:300]}
+        res[name]["wall_s"] = time.perf_counter() - t0
+    return res
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -611,7 +678,7 @@ def main():
 
     precision = fs.FP32 if args.precision == "fp32" else fs.FP64
     tmp = tempfile.mkdtemp(prefix="fdf_bench_%d_" % rank)
-    nsteps_total = args.warmup + args.steps + max(args.e2e_steps, 0) + 10
+    nsteps_total = args.warmup + args.steps + max(args.e2e_steps, 100, 5 * args.steps) + 30
     infile, prob = build_problem(tmp, nsteps_total, **(WORKLOAD if args.size == "full" else PROFILE_WORKLOAD))
     t_setup = time.perf_counter()
     p = fs.Problem(infile, precision=precision, device=local)
@@ -648,9 +715,12 @@ def main():
     value = node_stages / (ms * 1e-3)
 
     # end to end through the C-ABI with host buffers: upload the state from
-    # pinned host memory, then per step read back the on-fault output arrays
-    # that the reference's output units write every step (V, U, S, Sn, Vx, Sx)
-    ke = args.e2e_steps if args.e2e_steps > 0 else max(10, args.steps // 4)
+    # pinned host memory once, then run a stretch of the workload reading back
+    # after every step, into preallocated pinned buffers, the on-fault output
+    # arrays that the reference's output units write every step (V, U, S, Sn,
+    # Vx, Sx); the upload is counted in the timed region and spread over the
+    # steps in h2d_bytes_per_step
+    ke = args.e2e_steps if args.e2e_steps > 0 else max(100, 5 * args.steps)
     fields = [torch.empty(nodes, dtype=torch.float64, pin_memory=True) for _ in range(p.nfields)]
     for c in range(p.nfields):
         fields[c].numpy()[:] = p.field(c)
@@ -664,10 +734,11 @@ def main():
     t0 = time.perf_counter()
     for c in range(p.nfields):
         p.set_field(c, fields[c].numpy())
+    views = {w: o.numpy() for w, o in outs.items()}
     for _ in range(ke):
         p.step(1)
-        for w, o in outs.items():
-            o.numpy()[:] = p.fault(0, w)
+        for w, o in views.items():
+            p.fault(0, w, out=o)
     p.synchronize()
     te = time.perf_counter() - t0
     e2e_work, te = replicas.reduce_totals(float(nodes * nstages * ke), te, device="cuda")
@@ -692,18 +763,21 @@ def main():
     out = {"metric": METRIC, "value": value, "unit": "node-stage/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32" if precision == fs.FP32 else "f64", "data": "synthetic",
-           "config": {"workload": "planar3d: 2 blocks 401x201x201, slip weakening, log-normal mus, RK3",
+           "config": {"workload": PLANAR_WORKLOAD_NAME if args.size == "full" else "planar3d profile size 2x201x201x201",
                       "nodes": nodes, "stages_per_step": nstages, "l2": "inputs larger than L2 (5.96 GB/stage)",
                       "parallelism": "replicas" if world > 1 else "single", "setup_s": t_setup},
            "clocks": clk,
            "e2e": {"value": e2e, "unit": "node-stage/s", "h2d_bytes_per_step": h2d / ke, "d2h_bytes_per_step": d2h,
-                   "steps": ke, "note": "state uploaded once from pinned host memory (bytes amortised per step); "
-                                        "on-fault output arrays read back every step"},
+                   "steps": ke, "note": "state uploaded once from pinned host memory (bytes spread over the "
+                                        "steps); on-fault output arrays read back into pinned buffers after "
+                                        "every step"},
            "gpu_launches": launches,
            "kernel_ms": {"volume_avg": vol_avg_ms, "volume_launches": vol_n,
                          "interface_avg_per_stage": if_ms / max(if_n, 1)},
            "roofline": roofline}
     p.close()
+    if rank == 0 and world == 1 and args.size == "full" and not args.no_extras:
+        out["extras"] = run_extras()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, kind, cores, secs = cpu_reference_sample(tempfile.mkdtemp(prefix="fdf_cpu_"), 16, cpu_workers())
         out["cpu_baseline"] = {"value": rate, "unit": "node-stage/s", "cores": cores, "kind": kind,

@@ -295,8 +295,11 @@ class Problem:
         return b.value
 
     # --- state access --------------------------------------------------
-    def field(self, comp: int, absolute: bool = False) -> np.ndarray:
-        out = np.empty(self.nxyz)
+    def field(self, comp: int, absolute: bool = False, out: Optional[np.ndarray] = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.nxyz)
+        elif out.dtype != np.float64 or out.size != self.nxyz or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float64 array of %d values" % self.nxyz)
         self._check(self._L.fdf_get_field(self._h, comp, int(absolute), _dptr(out)))
         return out
 
@@ -331,11 +334,17 @@ class Problem:
         self._check(self._L.fdf_fault_count(self._h, iface, which, ctypes.byref(n)))
         return n.value
 
-    def fault(self, iface: int, which: int) -> Optional[np.ndarray]:
+    def fault(self, iface: int, which: int, out: Optional[np.ndarray] = None) -> Optional[np.ndarray]:
+        """Fault array `which` of interface `iface`; written into `out` (a
+        contiguous float64 array of the right size, e.g. a view of pinned host
+        memory) when given."""
         n = self.fault_count(iface, which)
         if n == 0:
             return None
-        out = np.empty(n)
+        if out is None:
+            out = np.empty(n)
+        elif out.dtype != np.float64 or out.size != n or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float64 array of %d values" % n)
         self._check(self._L.fdf_get_fault(self._h, iface, which, _dptr(out)))
         return out
 
