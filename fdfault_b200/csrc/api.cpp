@@ -271,6 +271,11 @@ int fdf_set_volume_kernel(fdf_handle* h, int kind, int* active) {
     });
 }
 
+int fdf_energy(fdf_handle* h, int with_rate, double out[8]) {
+    if (!out) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { s.energy(with_rate != 0, out); });
+}
+
 int fdf_set_wait_limit(fdf_handle* h, long long polls) {
     return guarded(h, [&](fdf::Solver& s) { s.set_wait_limit(polls); });
 }

@@ -13,6 +13,7 @@
 #include <stdexcept>
 #include <unordered_map>
 
+#include "energy.hpp"
 #include "noalloc.hpp"
 #include "output.hpp"
 
@@ -260,6 +261,7 @@ Solver::~Solver() {
     free_staged_maps(staged_maps_);
     free_reg_maps(reg_maps_);
     if (step_dev_) cudaFree(step_dev_);
+    if (energy_dev_) cudaFree(energy_dev_);
     mlp_free(mlp_);
     if (stz_counts_) cudaFree(stz_counts_);
     if (samples_) cudaFree(samples_);
@@ -1019,6 +1021,45 @@ void Solver::solve() {
 }
 
 void Solver::synchronize() { cuda_check(cudaStreamSynchronize(stream_), "synchronize"); }
+
+void Solver::energy(bool with_rate, double out[8]) {
+    if (P_.plastic()) throw std::runtime_error("energy diagnostics cover elastic problems only");
+    if (with_rate) {
+        // L(f) at the current state: stage 0 (A = 0 in every RK scheme) with
+        // dt = 1 and B = 0, so the new fields equal the old ones, slip and
+        // state do not move, and the rate register holds L(f)
+        const double b0 = B_[0];
+        B_[0] = 0.;
+        try {
+            if (precision_ == 0)
+                stage_impl<double>(1.0, 0, (double)step_index_ * dt_, false);
+            else
+                stage_impl<float>(1.0, 0, (double)step_index_ * dt_, false);
+        } catch (...) {
+            B_[0] = b0;
+            throw;
+        }
+        B_[0] = b0;
+        cuda_check(cudaGetLastError(), "energy rate stage");
+    }
+    if (!energy_dev_) cuda_check(cudaMalloc(&energy_dev_, 8 * sizeof(double)), "cudaMalloc energy accumulators");
+    cuda_check(cudaMemsetAsync(energy_dev_, 0, 8 * sizeof(double), stream_), "memset");
+    const double* Jd = (precision_ == 0) ? (const double*)J_ : J64_;
+    const double* Md = (precision_ == 0) ? (const double*)M_ : M64_;
+    for (const auto& B : blocks_) {
+        if (precision_ == 0) {
+            EnergyArgs<double> a{L_, (const double*)F_[cur_], with_rate ? (const double*)DF_ : nullptr, Jd};
+            launch_energy<double>(a, B, P_.sbporder, energy_dev_, stream_);
+        } else {
+            EnergyArgs<float> a{L_, (const float*)F_[cur_], with_rate ? (const float*)DF_ : nullptr, Jd};
+            launch_energy<float>(a, B, P_.sbporder, energy_dev_, stream_);
+        }
+    }
+    for (const auto& I : ifaces_)
+        if (I.kind >= 1) launch_fault_power(L_, I, blocks_[I.b1], P_.sbporder, Jd, Md, energy_dev_ + 4, stream_);
+    cuda_check(cudaGetLastError(), "energy launch");
+    fetch_to(energy_dev_, 8 * sizeof(double), out);
+}
 
 int Solver::check_status() {
     int st = 0;

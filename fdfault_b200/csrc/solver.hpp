@@ -66,6 +66,13 @@ class Solver {
     void refresh_stz() { synchronize(); update_stz_aux(); }   // after the network's buffers change
     void mlp_train_on_samples(int epochs, int batch, float lr, unsigned long long seed, double* tr, double* va);
 
+    // FP64 energy diagnostics (elastic problems): out[0] kinetic, out[1] strain
+    // energy, out[2] their rate under the semi-discrete operator at the current
+    // state (with_rate; computed by a stage evaluation that leaves fields, slip
+    // and state unchanged and the rate L(f) in the rate register), out[3] the
+    // sum of the rate terms' magnitudes, out[4] the frictional power of all
+    // interfaces, out[5..7] zero
+    void energy(bool with_rate, double out[8]);
     void synchronize();
     int check_status();            // reads and clears the device status word
     float time_steps(int nsteps);  // device time of nsteps steps, ms (CUDA events on the solver stream)
@@ -138,6 +145,7 @@ class Solver {
     StagedMapsHost* staged_maps_ = nullptr;   // tensor maps of the FP32 arrays (staged kernel)
     RegMapsHost* reg_maps_ = nullptr;         // tensor maps of the FP32 arrays (register-window kernel)
     long long wait_limit_ = 1LL << 22;        // polls of a bounded mbarrier wait (TMA-staged kernels)
+    double* energy_dev_ = nullptr;            // 8 FP64 accumulators of the energy diagnostics
 
     // device buffers
     void* F_[2] = {nullptr, nullptr};

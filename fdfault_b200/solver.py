@@ -70,6 +70,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fdf_use_fast_kernel.argtypes = [ctypes.c_void_p, c_int, P(c_int)]
     L.fdf_set_volume_kernel.argtypes = [ctypes.c_void_p, c_int, P(c_int)]
     L.fdf_set_wait_limit.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
+    L.fdf_energy.argtypes = [ctypes.c_void_p, c_int, P(ctypes.c_double)]
     L.fdf_use_graphs.argtypes = [ctypes.c_void_p, c_int]
     L.fdf_bytes_per_node_stage.argtypes = [ctypes.c_void_p, P(c_ll)]
     fp = P(ctypes.c_float)
@@ -278,6 +279,17 @@ class Problem:
         act = ctypes.c_int()
         self._check(self._L.fdf_set_volume_kernel(self._h, kind, ctypes.byref(act)))
         return act.value
+
+    def energy(self, rate: bool = True) -> dict:
+        """FP64 energy diagnostics (elastic problems): kinetic and strain energy
+        in the SBP norm, with `rate` their rate under the semi-discrete operator
+        at the current state (the state does not move; the rate register is left
+        holding L(f)) and the rate terms' magnitude sum, and the interfaces'
+        frictional power."""
+        out = (ctypes.c_double * 8)()
+        self._check(self._L.fdf_energy(self._h, int(rate), out))
+        return {"kinetic": out[0], "strain": out[1], "total": out[0] + out[1], "rate": out[2],
+                "rate_scale": out[3], "friction_power": out[4]}
 
     def set_wait_limit(self, polls: int) -> None:
         """Polls of each bounded wait for staged data in volume kernels 2 and 3

@@ -165,6 +165,25 @@ int fdf_set_volume_kernel(fdf_handle* h, int kind, int* active);
  * counterpart: the reference has no device waits. */
 int fdf_set_wait_limit(fdf_handle* h, long long polls);
 
+/* FP64 energy diagnostics of an elastic problem, accumulated on the device
+ * whatever the field precision, in the diagonal norm H of the SBP operator
+ * (H D + D^T H = diag(-1, 0, ..., 0, 1); its first entry is the reference's
+ * boundary norm h0, src/fd.cpp:119-120):
+ *   out[0] kinetic energy  sum w J rho |v|^2 / 2,
+ *   out[1] strain energy   sum w J sigma:S:sigma / 2   (w = H_i H_j H_k dxi dxeta dzeta),
+ *   out[2] (with_rate) dE/dt = sum w J (rho v.L_v + sigma:S:L_sigma) under the
+ *          semi-discrete operator L at the current state, volume terms, outer
+ *          SATs and interfaces together; L(f) is obtained by a stage evaluation
+ *          that leaves fields, slip and state unchanged and leaves L(f) in the
+ *          rate register (fdf_get_rate); call it between steps,
+ *   out[3] (with_rate) sum of the magnitudes of those rate terms (a scale),
+ *   out[4] frictional power of all interfaces: minus-side face area element
+ *          times traction . slip rate, from the fault arrays,
+ *   out[5..7] zero.
+ * Plastic problems are rejected.  No reference counterpart: the reference has
+ * no energy diagnostics. */
+int fdf_energy(fdf_handle* h, int with_rate, double out[8]);
+
 /* Algorithmic bytes moved per node per stage by the volume kernel. */
 int fdf_bytes_per_node_stage(fdf_handle* h, long long* bytes);
 
