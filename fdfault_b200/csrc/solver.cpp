@@ -1025,16 +1025,17 @@ void Solver::synchronize() { cuda_check(cudaStreamSynchronize(stream_), "synchro
 void Solver::energy(bool with_rate, double out[8]) {
     if (P_.plastic()) throw std::runtime_error("energy diagnostics cover elastic problems only");
     if (with_rate) {
-        // L(f) at the current state: stage 0 (A = 0 in every RK scheme) with
-        // dt = 1 and B = 0, so the new fields equal the old ones, slip and
-        // state do not move, and the rate register holds L(f)
+        // dt L(f) at the current state: stage 0 (A = 0 in every RK scheme)
+        // with B = 0, so the new fields equal the old ones, slip and state do
+        // not move, and the rate register holds dt L(f) (the volume
+        // coefficients carry the problem's dt, so the stage uses it too)
         const double b0 = B_[0];
         B_[0] = 0.;
         try {
             if (precision_ == 0)
-                stage_impl<double>(1.0, 0, (double)step_index_ * dt_, false);
+                stage_impl<double>(dt_, 0, (double)step_index_ * dt_, false);
             else
-                stage_impl<float>(1.0, 0, (double)step_index_ * dt_, false);
+                stage_impl<float>(dt_, 0, (double)step_index_ * dt_, false);
         } catch (...) {
             B_[0] = b0;
             throw;
@@ -1059,6 +1060,8 @@ void Solver::energy(bool with_rate, double out[8]) {
         if (I.kind >= 1) launch_fault_power(L_, I, blocks_[I.b1], P_.sbporder, Jd, Md, energy_dev_ + 4, stream_);
     cuda_check(cudaGetLastError(), "energy launch");
     fetch_to(energy_dev_, 8 * sizeof(double), out);
+    out[2] /= dt_;   // the register holds dt L(f)
+    out[3] /= dt_;
 }
 
 int Solver::check_status() {

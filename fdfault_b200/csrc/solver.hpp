@@ -69,7 +69,7 @@ class Solver {
     // FP64 energy diagnostics (elastic problems): out[0] kinetic, out[1] strain
     // energy, out[2] their rate under the semi-discrete operator at the current
     // state (with_rate; computed by a stage evaluation that leaves fields, slip
-    // and state unchanged and the rate L(f) in the rate register), out[3] the
+    // and state unchanged and dt L(f) in the rate register), out[3] the
     // sum of the rate terms' magnitudes, out[4] the frictional power of all
     // interfaces, out[5..7] zero
     void energy(bool with_rate, double out[8]);

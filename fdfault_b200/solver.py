@@ -284,7 +284,7 @@ class Problem:
         """FP64 energy diagnostics (elastic problems): kinetic and strain energy
         in the SBP norm, with `rate` their rate under the semi-discrete operator
         at the current state (the state does not move; the rate register is left
-        holding L(f)) and the rate terms' magnitude sum, and the interfaces'
+        holding dt L(f)) and the rate terms' magnitude sum, and the interfaces'
         frictional power."""
         out = (ctypes.c_double * 8)()
         self._check(self._L.fdf_energy(self._h, int(rate), out))

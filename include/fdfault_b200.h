@@ -174,8 +174,8 @@ int fdf_set_wait_limit(fdf_handle* h, long long polls);
  *   out[2] (with_rate) dE/dt = sum w J (rho v.L_v + sigma:S:L_sigma) under the
  *          semi-discrete operator L at the current state, volume terms, outer
  *          SATs and interfaces together; L(f) is obtained by a stage evaluation
- *          that leaves fields, slip and state unchanged and leaves L(f) in the
- *          rate register (fdf_get_rate); call it between steps,
+ *          that leaves fields, slip and state unchanged and leaves dt L(f) in
+ *          the rate register (fdf_get_rate); call it between steps,
  *   out[3] (with_rate) sum of the magnitudes of those rate terms (a scale),
  *   out[4] frictional power of all interfaces: minus-side face area element
  *          times traction . slip rate, from the fault arrays,

@@ -2,7 +2,8 @@
 
 * The device reductions (kinetic and strain energy in the SBP norm, their rate
   along the semi-discrete operator's L(f)) equal the same sums done here in
-  numpy from the fields, the rates the call leaves in the rate register and
+  numpy from the fields, the rates the call leaves in the rate register (dt
+  L(f)) and
   the Jacobian; the norm used here is re-derived from the closure rows of the
   reference's operator (src/fd.cpp:53-120) by the SBP property
   H D + D^T H = diag(-1, 0, ..., 0, 1) starting from its h0.
@@ -125,7 +126,7 @@ def test_energy_reductions_match_numpy(tmp_path, name):
         p.step(6)
         e = p.energy(rate=True)
         F = np.array([p.field(c) for c in range(p.nfields)])
-        R = np.array([p.rate(c) for c in range(p.nfields)])
+        R = np.array([p.rate(c) for c in range(p.nfields)]) / p.dt   # the register holds dt L(f)
         J = p.geometry(2)
     k, s, r, scale = energy_numpy(prob, J, F, R)
     assert abs(e["kinetic"] - k) <= 1e-12 * abs(k)
