@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(256) k_energy(EnergyArgs<T> a, BlockDev B, Nor
         const int k = (int)(t % n2), j = (int)((t / n2) % n1), i = (int)(t / ((long long)n2 * n1));
         const long long id = (L.ndim == 3) ? node_index(L, B.lo[0] + i, B.lo[1] + j, B.lo[2] + k)
                                            : node_index(L, B.lo[0] + i, B.lo[1] + j, 0);
-        double w = hw(W, i, n0) * hw(W, j, n1) * B.dx[0] * B.dx[1] * a.J[id];
+        double w = hw(W, i, n0) * hw(W, j, n1) * B.dx[0] * B.dx[1] * (double)a.J[id];
         if (L.ndim == 3) w *= hw(W, k, n2) * B.dx[2];
         double v[3] = {0., 0., 0.}, rv[3] = {0., 0., 0.}, s[6] = {0., 0., 0., 0., 0., 0.}, rs[6] = {0., 0., 0., 0., 0., 0.};
         auto f = [&](int c) { return (double)a.F[c * cs + id]; };
@@ -130,8 +130,9 @@ __global__ void __launch_bounds__(256) k_energy(EnergyArgs<T> a, BlockDev B, Nor
 
 // frictional power on one interface: sum over its nodes of the face area
 // element (minus side) times traction . slip rate
-__global__ void __launch_bounds__(256) k_fault_power(Layout L, IfaceDev I, BlockDev B1, NormW W, const double* J,
-                                                     const double* M, double* out) {
+template <typename T>
+__global__ void __launch_bounds__(256) k_fault_power(Layout L, IfaceDev I, BlockDev B1, NormW W, const T* J,
+                                                     const T* M, double* out) {
     const int nf = I.n0 * I.n1;
     const int D = I.direction;
     const int o0 = (D == 0) ? 1 : 0, o1 = (D == 2) ? 1 : 2;
@@ -144,10 +145,10 @@ __global__ void __launch_bounds__(256) k_fault_power(Layout L, IfaceDev I, Block
         const long long id = (L.ndim == 3) ? node_index(L, g[0], g[1], g[2]) : node_index(L, g[0], g[1], 0);
         double gn = 0.;
         for (int m = 0; m < L.ndim; m++) {
-            const double q = M[(D * L.ndim + m) * L.cstride + id];
+            const double q = (double)M[(D * L.ndim + m) * L.cstride + id];
             gn += q * q;
         }
-        double w = J[id] * sqrt(gn) * hw(W, a, B1.n[o0]) * B1.dx[o0];
+        double w = (double)J[id] * sqrt(gn) * hw(W, a, B1.n[o0]) * B1.dx[o0];
         if (L.ndim == 3) w *= hw(W, b, B1.n[o1]) * B1.dx[o1];
         double sv = 0.;
         for (int c = 0; c < L.ndim - 1; c++) sv += I.sx[c * nf + t] * I.vx[c * nf + t];
@@ -172,14 +173,20 @@ void launch_energy(const EnergyArgs<T>& a, const BlockDev& b, int order, double*
 template void launch_energy<float>(const EnergyArgs<float>&, const BlockDev&, int, double*, cudaStream_t);
 template void launch_energy<double>(const EnergyArgs<double>&, const BlockDev&, int, double*, cudaStream_t);
 
-void launch_fault_power(const Layout& L, const IfaceDev& I, const BlockDev& b1, int order, const double* J,
-                        const double* M, double* out, cudaStream_t s) {
+template <typename T>
+void launch_fault_power(const Layout& L, const IfaceDev& I, const BlockDev& b1, int order, const T* J, const T* M,
+                        double* out, cudaStream_t s) {
     NormW W;
     norm_weights(order, W.h, &W.nb);
     const int nf = I.n0 * I.n1;
     int grid = (nf + 255) / 256;
     if (grid > 1024) grid = 1024;
-    k_fault_power<<<grid, 256, 0, s>>>(L, I, b1, W, J, M, out);
+    k_fault_power<T><<<grid, 256, 0, s>>>(L, I, b1, W, J, M, out);
 }
+
+template void launch_fault_power<float>(const Layout&, const IfaceDev&, const BlockDev&, int, const float*,
+                                        const float*, double*, cudaStream_t);
+template void launch_fault_power<double>(const Layout&, const IfaceDev&, const BlockDev&, int, const double*,
+                                         const double*, double*, cudaStream_t);
 
 }  // namespace fdf

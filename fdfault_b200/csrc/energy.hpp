@@ -15,7 +15,7 @@ struct EnergyArgs {
     Layout L;
     const T* F;        // fields
     const T* R;        // rates L(f), or null
-    const double* J;   // Jacobian (FP64)
+    const T* J;        // Jacobian
 };
 
 // adds kinetic energy, strain energy, their rate along R and the sum of the
@@ -23,8 +23,9 @@ struct EnergyArgs {
 template <typename T>
 void launch_energy(const EnergyArgs<T>& a, const BlockDev& b, int order, double* out, cudaStream_t s);
 // adds the frictional power (face area element x traction . slip rate) of
-// interface I to out[0]; J, M the FP64 Jacobian and metric
-void launch_fault_power(const Layout& L, const IfaceDev& I, const BlockDev& b1, int order, const double* J,
-                        const double* M, double* out, cudaStream_t s);
+// interface I to out[0]; J, M the Jacobian and metric
+template <typename T>
+void launch_fault_power(const Layout& L, const IfaceDev& I, const BlockDev& b1, int order, const T* J, const T* M,
+                        double* out, cudaStream_t s);
 
 }  // namespace fdf

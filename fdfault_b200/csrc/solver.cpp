@@ -1045,19 +1045,28 @@ void Solver::energy(bool with_rate, double out[8]) {
     }
     if (!energy_dev_) cuda_check(cudaMalloc(&energy_dev_, 8 * sizeof(double)), "cudaMalloc energy accumulators");
     cuda_check(cudaMemsetAsync(energy_dev_, 0, 8 * sizeof(double), stream_), "memset");
-    const double* Jd = (precision_ == 0) ? (const double*)J_ : J64_;
-    const double* Md = (precision_ == 0) ? (const double*)M_ : M64_;
+    // geometry in the fields' precision (FP32 problems keep no FP64 copy after set-up)
+    if (!J_ || !M_ || !F_[cur_] || !DF_) throw std::runtime_error("energy diagnostics: arrays not allocated");
     for (const auto& B : blocks_) {
         if (precision_ == 0) {
-            EnergyArgs<double> a{L_, (const double*)F_[cur_], with_rate ? (const double*)DF_ : nullptr, Jd};
+            EnergyArgs<double> a{L_, (const double*)F_[cur_], with_rate ? (const double*)DF_ : nullptr,
+                                 (const double*)J_};
             launch_energy<double>(a, B, P_.sbporder, energy_dev_, stream_);
         } else {
-            EnergyArgs<float> a{L_, (const float*)F_[cur_], with_rate ? (const float*)DF_ : nullptr, Jd};
+            EnergyArgs<float> a{L_, (const float*)F_[cur_], with_rate ? (const float*)DF_ : nullptr,
+                                (const float*)J_};
             launch_energy<float>(a, B, P_.sbporder, energy_dev_, stream_);
         }
     }
-    for (const auto& I : ifaces_)
-        if (I.kind >= 1) launch_fault_power(L_, I, blocks_[I.b1], P_.sbporder, Jd, Md, energy_dev_ + 4, stream_);
+    for (const auto& I : ifaces_) {
+        if (I.kind < 1) continue;
+        if (precision_ == 0)
+            launch_fault_power<double>(L_, I, blocks_[I.b1], P_.sbporder, (const double*)J_, (const double*)M_,
+                                       energy_dev_ + 4, stream_);
+        else
+            launch_fault_power<float>(L_, I, blocks_[I.b1], P_.sbporder, (const float*)J_, (const float*)M_,
+                                      energy_dev_ + 4, stream_);
+    }
     cuda_check(cudaGetLastError(), "energy launch");
     fetch_to(energy_dev_, 8 * sizeof(double), out);
     out[2] /= dt_;   // the register holds dt L(f)
