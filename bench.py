@@ -304,10 +304,14 @@ def run_stz(args, local):
         params = p.mlp_params()
     runs = {}
     keys = (fs.U, fs.V, fs.S, fs.STATE)
-    for mode in ("plain", "learned"):
+    # the learned start and its judges: the reference's midpoint start, a warm
+    # start from each node's previous root, and the exact derivative
+    starts = {"plain": fs.Problem.STZ_MIDPOINT, "learned": fs.Problem.STZ_LEARNED, "warm": fs.Problem.STZ_WARM,
+              "exact_derivative": fs.Problem.STZ_EXACT_DERIVATIVE}
+    for mode, code in starts.items():
         with fs.Problem(infile, precision=fs.FP32, device=local) as q:
             q.mlp_set_params(params)
-            q.stz_learned(mode == "learned")
+            q.stz_start(code)
             q.step(args.warmup)
             q.synchronize()
             q.profile(True)
@@ -344,7 +348,9 @@ def run_stz(args, local):
                                   % (size["nx"], size["ny"], size["nz"]), "nodes": nodes},
            "training": {"samples": cnt, "collected_over_steps": ncollect, "epochs": epochs, "seconds": train_s,
                         "train_loss": tr, "heldout_loss": va},
-           "plain": runs["plain"], "learned": runs["learned"], "learned_vs_plain_rel_l2": learned_vs_plain}
+           "plain": runs["plain"], "learned": runs["learned"],
+           "judges": {"warm": runs["warm"], "exact_derivative": runs["exact_derivative"]},
+           "learned_vs_plain_rel_l2": learned_vs_plain}
     print(json.dumps(out), flush=True)
 
 

@@ -63,6 +63,12 @@ struct MlpDev {
 // STZ Newton counters and solver-generated training samples (both optional)
 struct StzAux {
     int learned;                       // 1: start Newton from the network's guess
+    // start of the plain solve when not learned: 0 bracket midpoint with the
+    // reference's derivative; 2 warm start (this node's previous converged mu,
+    // mu_prev) with the reference's derivative; 3 bracket midpoint with the
+    // exact derivative of the slip-rate law
+    int start;
+    double* mu_prev;                   // per fault node, < 0 where none yet (start 2)
     MlpDev mlp;
     unsigned long long* stats;         // [0] Newton solves, [1] iterations, [2] starts from the midpoint
     float* samples;                    // [cap][8]: 6 inputs, target logit(s)/20, converged mu

@@ -90,10 +90,15 @@ __device__ __forceinline__ double stz_func(double mu, const StzPar& p) {
     return p.eta * stz_vpl(mu, p) - p.snc * mu - p.phi;
 }
 __device__ __forceinline__ double stz_der(double mu, const StzPar& p) { return p.eta * stz_dvpldmu(mu, p) - p.snc; }
+// exact derivative of the root function: dV/dmu = V (1/a + muy / (mu (mu - muy)))
+__device__ __forceinline__ double stz_der_exact(double mu, const StzPar& p) {
+    const double dv = (mu <= p.muy) ? 0. : stz_vpl(mu, p) * (1. / p.a + p.muy / mu / (mu - p.muy));
+    return p.eta * dv - p.snc;
+}
 
 // bracketed Newton with bisection fallback; returns a status bit on failure and
 // the number of iterations taken in *iters
-__device__ int solve_newton(double xmin, double xmax, const StzPar& p, double* out, int* iters) {
+__device__ int solve_newton(double xmin, double xmax, const StzPar& p, double* out, int* iters, bool exact = false) {
     const int nmax = 100;
     const double tol = 2.e-16;
     double func, der, x, xl, xh, fh, dx, dxold, temp;
@@ -129,7 +134,7 @@ __device__ int solve_newton(double xmin, double xmax, const StzPar& p, double* o
     }
     x = 0.5 * (xh + xl);
     func = stz_func(x, p);
-    der = stz_der(x, p);
+    der = exact ? stz_der_exact(x, p) : stz_der(x, p);
     dx = fabs(xh - xl);
     dxold = dx;
     int i = 0;
@@ -153,7 +158,7 @@ __device__ int solve_newton(double xmin, double xmax, const StzPar& p, double* o
         }
         if (fabs(dx) < tol) break;
         func = stz_func(x, p);
-        der = stz_der(x, p);
+        der = exact ? stz_der_exact(x, p) : stz_der(x, p);
         if (func < 0.)
             xl = x;
         else
@@ -170,7 +175,8 @@ __device__ int solve_newton(double xmin, double xmax, const StzPar& p, double* o
 // of f(x0) (a guess where f overflows becomes the new upper end and the start
 // moves to the midpoint, as in the plain solve).  Returns FDF_ERR_NEWTON if it
 // does not converge; the caller then falls back to the plain solve.
-__device__ int solve_newton_from(double xmin, double xmax, double x0, const StzPar& p, double* out, int* iters) {
+__device__ int solve_newton_from(double xmin, double xmax, double x0, const StzPar& p, double* out, int* iters,
+                                 bool exact = false) {
     const int nmax = 100;
     const double tol = 2.e-16;
     double xl = xmin, xh = xmax, x = x0;
@@ -190,7 +196,7 @@ __device__ int solve_newton_from(double xmin, double xmax, double x0, const StzP
         xl = x;
     else
         xh = x;
-    double der = stz_der(x, p);
+    double der = exact ? stz_der_exact(x, p) : stz_der(x, p);
     double dx = fabs(xh - xl), dxold = dx, temp;
     int i = 0;
     while (i < nmax) {
@@ -209,7 +215,7 @@ __device__ int solve_newton_from(double xmin, double xmax, double x0, const StzP
         }
         if (fabs(dx) < tol) break;
         func = stz_func(x, p);
-        der = stz_der(x, p);
+        der = exact ? stz_der_exact(x, p) : stz_der(x, p);
         if (func < 0.)
             xl = x;
         else
@@ -382,13 +388,27 @@ __device__ int solve_fs(const IfaceDev& I, double phi, double eta, double snc, l
                 p.a += I.par[2][ij];
                 p.muy += I.par[3][ij];
             }
-            if (p.muy >= -phi / snc) {
-                mu = -phi / snc;
+            const double mh = -phi / snc;
+            if (p.muy >= mh) {
+                mu = mh;
             } else {
-                int iters = 0;
-                const int s1 = solve_newton(p.muy, -phi / snc, p, &mu, &iters);
+                int iters = 0, s1 = FDF_ERR_NEWTON;
+                bool midpoint = true;
+                if (I.stz.start == 2 && I.stz.mu_prev) {   // warm start from this node's last root
+                    const double x0 = I.stz.mu_prev[ij];
+                    if (x0 > p.muy && x0 < mh) {
+                        s1 = solve_newton_from(p.muy, mh, x0, p, &mu, &iters);
+                        midpoint = s1 != 0;
+                    }
+                }
+                if (s1 != 0) {
+                    int it2 = 0;
+                    s1 = solve_newton(p.muy, mh, p, &mu, &it2, I.stz.start == 3);
+                    iters += it2;
+                }
                 st |= s1;
-                if (I.stz.stats || I.stz.samples) stz_record(I, p, mu, iters, true, s1, nullptr);
+                if (I.stz.start == 2 && I.stz.mu_prev) I.stz.mu_prev[ij] = mu;
+                if (I.stz.stats || I.stz.samples) stz_record(I, p, mu, iters, midpoint, s1, nullptr);
             }
         }
         if (mu * fabs(snc) > phi) {

@@ -262,6 +262,7 @@ Solver::~Solver() {
     free_reg_maps(reg_maps_);
     if (step_dev_) cudaFree(step_dev_);
     if (energy_dev_) cudaFree(energy_dev_);
+    if (stz_mu_prev_) cudaFree(stz_mu_prev_);
     mlp_free(mlp_);
     if (stz_counts_) cudaFree(stz_counts_);
     if (samples_) cudaFree(samples_);
@@ -1147,15 +1148,45 @@ void Solver::get_field_noalloc(int comp, bool absolute, double* out) {
 
 void Solver::update_stz_aux() {
     graph_dirty_ = true;
+    long long off = 0;
     for (auto& I : ifaces_) {
         if (I.kind != 3) continue;
         I.stz.learned = stz_learned_ ? 1 : 0;
+        I.stz.start = stz_start_;
+        I.stz.mu_prev = (stz_start_ == 2 && stz_mu_prev_) ? stz_mu_prev_ + off : nullptr;
+        off += (long long)I.n0 * I.n1;
         I.stz.mlp = mlp_.ready ? mlp_.dev() : MlpDev{};
         I.stz.stats = stz_counting_ ? stz_counts_ : nullptr;
         I.stz.samples = samples_;
         I.stz.nsamples = nsamples_;
         I.stz.cap = sample_cap_;
     }
+}
+
+void Solver::set_stz_start(int mode) {
+    if (mode == 1) {
+        set_stz_learned(true);
+        return;
+    }
+    if (mode != 0 && mode != 2 && mode != 3) throw std::invalid_argument("STZ start mode must be 0, 1, 2 or 3");
+    synchronize();
+    stz_learned_ = false;
+    stz_start_ = mode;
+    if (mode == 2) {   // one slot per node of every STZ interface, none known yet
+        long long total = 0;
+        for (const auto& I : ifaces_)
+            if (I.kind == 3) total += (long long)I.n0 * I.n1;
+        if (!stz_mu_prev_ && total > 0)
+            cuda_check(cudaMalloc(&stz_mu_prev_, total * sizeof(double)), "cudaMalloc warm-start roots");
+        if (stz_mu_prev_) {
+            std::vector<double> none((size_t)total, -1.);
+            cuda_check(cudaMemcpyAsync(stz_mu_prev_, none.data(), total * sizeof(double), cudaMemcpyHostToDevice,
+                                       stream_),
+                       "warm-start reset");
+            cuda_check(cudaStreamSynchronize(stream_), "warm-start reset");
+        }
+    }
+    update_stz_aux();
 }
 
 void Solver::set_stz_learned(bool on) {

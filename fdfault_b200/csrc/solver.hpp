@@ -58,6 +58,10 @@ class Solver {
 
     // STZ friction: learned Newton start, counters, solver-generated samples
     void set_stz_learned(bool on);
+    // start of the plain STZ Newton solve: 0 bracket midpoint (reference), 2
+    // warm start from each node's previous root, 3 midpoint with the exact
+    // derivative (1 is the learned start, set_stz_learned)
+    void set_stz_start(int mode);
     void set_stz_counting(bool on);
     void read_stz_counts(long long out[3], bool reset);
     void stz_collect(long long capacity);            // 0 stops collecting and frees the buffer
@@ -169,6 +173,8 @@ class Solver {
     std::vector<IfaceDev> ifaces_;
     MlpState mlp_;
     bool stz_learned_ = false;
+    int stz_start_ = 0;
+    double* stz_mu_prev_ = nullptr;   // per interface node of all STZ interfaces (warm start)
     unsigned long long* stz_counts_ = nullptr;   // device [3]
     bool stz_counting_ = false;
     float* samples_ = nullptr;                   // device [cap][8]

@@ -75,6 +75,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fdf_bytes_per_node_stage.argtypes = [ctypes.c_void_p, P(c_ll)]
     fp = P(ctypes.c_float)
     L.fdf_stz_set_learned.argtypes = [ctypes.c_void_p, c_int]
+    L.fdf_stz_set_start.argtypes = [ctypes.c_void_p, c_int]
     L.fdf_stz_set_counting.argtypes = [ctypes.c_void_p, c_int]
     L.fdf_stz_read_counts.argtypes = [ctypes.c_void_p, P(c_ll), c_int]
     L.fdf_stz_collect.argtypes = [ctypes.c_void_p, c_ll]
@@ -207,6 +208,14 @@ class Problem:
     # --- STZ friction: learned Newton start ------------------------------
     def stz_learned(self, on: bool) -> None:
         self._check(self._L.fdf_stz_set_learned(self._h, int(on)))
+
+    STZ_MIDPOINT, STZ_LEARNED, STZ_WARM, STZ_EXACT_DERIVATIVE = 0, 1, 2, 3
+
+    def stz_start(self, mode: int) -> None:
+        """Start of the STZ Newton solve: 0 bracket midpoint (reference), 1
+        learned, 2 warm start from each node's previous root, 3 midpoint with
+        the exact derivative."""
+        self._check(self._L.fdf_stz_set_start(self._h, mode))
 
     def stz_counting(self, on: bool) -> None:
         self._check(self._L.fdf_stz_set_counting(self._h, int(on)))

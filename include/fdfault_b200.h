@@ -203,6 +203,17 @@ int fdf_bytes_per_node_stage(fdf_handle* h, long long* bytes);
  * W1[64][6], b1[64], W2[64][64], b2[64], W3[64], b3. */
 #define FDF_MLP_NPARAM 4673
 int fdf_stz_set_learned(fdf_handle* h, int on);
+
+/* Start of the STZ Newton solve, for judging the learned start against other
+ * ways of cutting iterations: 0 bracket midpoint with the reference's
+ * derivative (the reference, src/utilities.cpp:97 and src/stz.cpp:479; the
+ * default), 1 the learned start (as fdf_stz_set_learned 1), 2 warm start from
+ * each node's previous converged mu (the previous stage's root; the midpoint
+ * where none is known or it leaves the bracket), 3 bracket midpoint with the
+ * exact derivative of the slip-rate law instead of the reference's (whose sign
+ * of the mu_y term makes the iteration converge linearly).  Modes 1-3 converge
+ * to the same roots within the Newton tolerance, not bit for bit. */
+int fdf_stz_set_start(fdf_handle* h, int mode);
 /* counters of the Newton solves: [0] solves, [1] iterations, [2] solves that
  * started at the bracket midpoint (plain, or a rejected guess) */
 int fdf_stz_set_counting(fdf_handle* h, int on);

@@ -149,3 +149,33 @@ def test_learned_start_matches_plain_and_saves_iterations(trained, precision):
     assert mid_p == nsol_p            # the plain solve always starts at the midpoint
     assert mid_l <= 0.02 * nsol_l     # the guess is rejected rarely
     assert it_l / nsol_l < 0.85 * it_p / nsol_p
+
+
+@pytest.mark.parametrize("precision", [fs.FP64, fs.FP32])
+def test_judge_starts_match_plain_and_count_iterations(trained, precision):
+    """The two other ways of cutting Newton iterations that judge the learned
+    start: a warm start from each node's previous root, and the exact
+    derivative of the slip-rate law (the reference's has the wrong sign on its
+    mu_y term).  Both converge to the plain solve's roots; the iteration counts
+    of all four starts are printed."""
+    nsteps = 20
+    modes = {"plain": fs.Problem.STZ_MIDPOINT, "learned": fs.Problem.STZ_LEARNED, "warm": fs.Problem.STZ_WARM,
+             "exact derivative": fs.Problem.STZ_EXACT_DERIVATIVE}
+    runs = {}
+    for mode, code in modes.items():
+        with fs.Problem(trained["infile"], precision=precision) as p:
+            p.mlp_set_params(trained["params"])
+            p.stz_start(code)
+            p.stz_counting(True)
+            p.step(nsteps)
+            r = {w: p.fault(0, w) for w in (fs.U, fs.V, fs.S, fs.STATE)}
+            r["counts"] = p.stz_counts()
+            runs[mode] = r
+    per = {m: runs[m]["counts"][1] / max(runs[m]["counts"][0], 1) for m in runs}
+    print("Newton iterations per solve:", {m: round(v, 3) for m, v in per.items()})
+    for m in ("warm", "exact derivative"):
+        for w in (fs.U, fs.V, fs.S, fs.STATE):
+            assert rel_l2(runs[m][w], runs["plain"][w]) <= 1e-5, (m, w)
+        assert runs[m]["counts"][0] == runs["plain"]["counts"][0]
+    assert per["exact derivative"] < per["plain"]
+    assert per["warm"] < per["plain"]
