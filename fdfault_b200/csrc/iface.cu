@@ -48,6 +48,37 @@ __global__ void k_fetch(Layout L, const T* __restrict__ F, int comp, int add_str
     out[t] = v;
 }
 
+// one output unit's window of a field component: out[(a*ny + b)*nz + c] =
+// F at node (xm0 + a xs0, xm1 + b xs1, xm2 + c xs2), plus the initial stress
+// when add_stress (the same conversion as k_fetch)
+template <typename T>
+__global__ void k_gather_window(Layout L, const T* __restrict__ F, int comp, int add_stress, double s0v,
+                                const double* __restrict__ S, int scomp, OutWindow w, double* __restrict__ out) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long nn = (long long)w.n[0] * w.n[1] * w.n[2];
+    if (t >= nn) return;
+    const int c = (int)(t % w.n[2]), b = (int)((t / w.n[2]) % w.n[1]), a = (int)(t / ((long long)w.n[2] * w.n[1]));
+    const long long id = node_index(L, w.xm[0] + a * w.xs[0], w.xm[1] + b * w.xs[1], w.xm[2] + c * w.xs[2]);
+    double v = (double)F[comp * L.cstride + id];
+    if (add_stress) {
+        v += s0v;
+        if (S) v += S[scomp * L.cstride + id];
+    }
+    out[t] = v;
+}
+
+// one output unit's window of a fault array (face node (p_a, p_b) at
+// offset + (p_a - base_a) * n1 + (p_b - base_b))
+__global__ void k_gather_fault(const double* __restrict__ arr, long long offset, int n1, int fa, int fb, int base_a,
+                               int base_b, OutWindow w, double* __restrict__ out) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long nn = (long long)w.n[0] * w.n[1] * w.n[2];
+    if (t >= nn) return;
+    const int c = (int)(t % w.n[2]), b = (int)((t / w.n[2]) % w.n[1]), a = (int)(t / ((long long)w.n[2] * w.n[1]));
+    const int pos[3] = {w.xm[0] + a * w.xs[0], w.xm[1] + b * w.xs[1], w.xm[2] + c * w.xs[2]};
+    out[t] = arr[offset + (long long)(pos[fa] - base_a) * n1 + (pos[fb] - base_b)];
+}
+
 template <typename T>
 __global__ void k_store(Layout L, T* __restrict__ F, int comp, const double* __restrict__ in) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -101,6 +132,27 @@ template void launch_fetch_component<double>(const Layout&, const double*, int, 
                                              double*, cudaStream_t);
 template void launch_fetch_component<float>(const Layout&, const float*, int, int, const double*, const double*,
                                             double*, cudaStream_t);
+
+template <typename T>
+void launch_gather_window(const Layout& L, const T* F, int comp, int add_stress, const double s0[6], const double* S,
+                          const OutWindow& w, double* out, cudaStream_t s) {
+    const long long nn = (long long)w.n[0] * w.n[1] * w.n[2];
+    int sc = comp - L.nv;
+    double s0v = (add_stress && sc >= 0 && sc < L.ns) ? s0[L.sidx[sc]] : 0.;
+    int add = add_stress && sc >= 0 && sc < L.ns;
+    k_gather_window<T><<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(L, F, comp, add, s0v, add ? S : nullptr, sc, w,
+                                                                      out);
+}
+template void launch_gather_window<double>(const Layout&, const double*, int, int, const double*, const double*,
+                                           const OutWindow&, double*, cudaStream_t);
+template void launch_gather_window<float>(const Layout&, const float*, int, int, const double*, const double*,
+                                          const OutWindow&, double*, cudaStream_t);
+
+void launch_gather_fault(const double* arr, long long offset, int n1, int fa, int fb, int base_a, int base_b,
+                         const OutWindow& w, double* out, cudaStream_t s) {
+    const long long nn = (long long)w.n[0] * w.n[1] * w.n[2];
+    k_gather_fault<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(arr, offset, n1, fa, fb, base_a, base_b, w, out);
+}
 
 template <typename T>
 void launch_store_component(const Layout& L, T* F, int comp, const double* in, cudaStream_t s) {

@@ -110,6 +110,14 @@ void launch_interface(const IfaceArgs<T>& a, const IfaceDev& itf, const BlockDev
                       const StageArgs& sa, int no_sat, cudaStream_t s);
 
 // output helpers
+struct OutWindow {   // strided index window of an output unit (global node indices)
+    int xm[3], xs[3], n[3];
+};
+template <typename T>
+void launch_gather_window(const Layout& L, const T* F, int comp, int add_stress, const double s0[6], const double* S,
+                          const OutWindow& w, double* out, cudaStream_t s);
+void launch_gather_fault(const double* arr, long long offset, int n1, int fa, int fb, int base_a, int base_b,
+                         const OutWindow& w, double* out, cudaStream_t s);
 template <typename T>
 void launch_fetch_component(const Layout& L, const T* F, int comp, int add_stress, const double s0[6],
                             const double* S, double* out, cudaStream_t s);

@@ -7,6 +7,7 @@
 #include <fstream>
 #include <stdexcept>
 
+#include "kernels.hpp"
 #include "solver.hpp"
 
 namespace fdf {
@@ -213,48 +214,99 @@ void OutputList::open_unit(Unit& u) {
     write_meta(base, u.field, (u.tp - u.tm) / u.ts + 1, u.nx);
 }
 
-void OutputList::write(int tstep) {
-    const ProblemSpec& P = S_.spec();
-    for (Unit& u : units_) {
-        if (tstep < u.tm || tstep > u.tp || (tstep - u.tm) % u.ts != 0) continue;
+void OutputList::enqueue(Unit& u, int tstep, double* dst) {
+    Solver& S = S_;
+    OutWindow w;
+    for (int i = 0; i < 3; i++) {
+        w.xm[i] = u.xm[i];
+        w.xs[i] = u.xs[i];
+        w.n[i] = u.nx[i];
+    }
+    if (u.location == -1) {
+        const Layout& L = S.L_;
+        const int comp = u.comp;
+        const bool stress = comp >= L.nv && comp < L.nv + L.ns;
+        if (stress && S.precision_ == 0 && tstep > 0 && S.ABS_) {
+            // absolute stresses of the step as the reference's output round trip left them
+            launch_gather_window<double>(L, S.ABS_, comp - L.nv, 0, S.P_.s0, nullptr, w, dst, S.stream_);
+        } else {
+            const bool plastic_field = comp >= L.nfields;
+            void* base = plastic_field ? S.FP_ : S.F_[S.cur_];
+            const int c = plastic_field ? comp - L.nfields : comp;
+            if (S.precision_ == 0)
+                launch_gather_window<double>(L, (const double*)base, c, !plastic_field, S.P_.s0, S.S_, w, dst,
+                                             S.stream_);
+            else
+                launch_gather_window<float>(L, (const float*)base, c, !plastic_field, S.P_.s0, S.S_, w, dst,
+                                            S.stream_);
+        }
+    } else {
+        const IfaceDev& D = S.ifaces()[u.location];
+        const int dir = D.direction;
+        const int a = (dir == 0) ? 1 : 0, b = (dir == 2) ? 1 : 2;
+        launch_gather_fault(S.fault_ptr(u.location, u.comp), u.offset, D.n1, a, b, D.mlb[a], D.mlb[b], w, dst,
+                            S.stream_);
+    }
+}
+
+void OutputList::flush(int slot) {
+    Slot& sl = slots_[slot];
+    if (!sl.pending) return;
+    if (cudaEventSynchronize(sl.done) != cudaSuccess) throw std::runtime_error("CUDA error waiting for output copy");
+    const double* h = hstage_ + (size_t)slot * cap_;
+    for (const auto& it : sl.items) {
+        Unit& u = units_[it.first];
         if (u.tfile) {
-            double t = (double)tstep * S_.dt();
+            const double t = (double)sl.tstep * S_.dt();
             std::fwrite(&t, sizeof(double), 1, u.tfile);
         }
-        if (u.location == -1) {
-            const size_t nall = (size_t)P.nx[0] * P.nx[1] * P.nx[2];
-            hbuf_.resize(nall);
-            S_.fetch_output_component(u.comp, tstep, hbuf_.data());
-            for (int i = 0; i < u.nx[0]; i++)
-                for (int j = 0; j < u.nx[1]; j++)
-                    for (int k = 0; k < u.nx[2]; k++) {
-                        size_t id = ((size_t)(u.xm[0] + i * u.xs[0]) * P.nx[1] + (u.xm[1] + j * u.xs[1])) * P.nx[2] +
-                                    (u.xm[2] + k * u.xs[2]);
-                        std::fwrite(&hbuf_[id], sizeof(double), 1, u.data);
-                    }
-        } else {
-            const IfaceDev& D = S_.ifaces()[u.location];
-            long long n = S_.fault_count(u.location, u.comp);
-            hbuf_.resize((size_t)n);
-            S_.get_fault(u.location, u.comp, hbuf_.data());
-            const int dir = D.direction;
-            const int a = (dir == 0) ? 1 : 0, b = (dir == 2) ? 1 : 2;
-            int base[3] = {D.mlb[0], D.mlb[1], D.mlb[2]};
-            for (int i = 0; i < u.nx[0]; i++)
-                for (int j = 0; j < u.nx[1]; j++)
-                    for (int k = 0; k < u.nx[2]; k++) {
-                        int pos[3] = {u.xm[0] + i * u.xs[0], u.xm[1] + j * u.xs[1], u.xm[2] + k * u.xs[2]};
-                        long long ij = (long long)(pos[a] - base[a]) * D.n1 + (pos[b] - base[b]);
-                        std::fwrite(&hbuf_[(size_t)(u.offset + ij)], sizeof(double), 1, u.data);
-                    }
-        }
-        std::fflush(u.data);
+        const size_t n = (size_t)u.nx[0] * u.nx[1] * u.nx[2];
+        if (std::fwrite(h + it.second, sizeof(double), n, u.data) != n)
+            throw std::runtime_error("Error writing output unit " + u.name);
     }
+    sl.pending = false;
+    sl.items.clear();
+}
+
+void OutputList::write(int tstep) {
+    std::vector<std::pair<int, size_t>> due;
+    size_t n = 0;
+    for (size_t i = 0; i < units_.size(); i++) {
+        const Unit& u = units_[i];
+        if (tstep < u.tm || tstep > u.tp || (tstep - u.tm) % u.ts != 0) continue;
+        due.push_back({(int)i, n});
+        n += (size_t)u.nx[0] * u.nx[1] * u.nx[2];
+    }
+    if (due.empty()) return;
+    if (!dstage_) {   // every unit's window fits in one slot
+        for (const Unit& u : units_) cap_ += (size_t)u.nx[0] * u.nx[1] * u.nx[2];
+        if (cudaMalloc(&dstage_, 2 * cap_ * sizeof(double)) != cudaSuccess ||
+            cudaMallocHost(&hstage_, 2 * cap_ * sizeof(double)) != cudaSuccess)
+            throw std::runtime_error("CUDA error allocating output staging");
+        for (Slot& sl : slots_)
+            if (cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess)
+                throw std::runtime_error("CUDA error creating output event");
+    }
+    const int slot = next_;
+    flush(slot);   // the slot's previous contents (two output steps ago) go to the files first
+    double* d = dstage_ + (size_t)slot * cap_;
+    for (const auto& it : due) enqueue(units_[it.first], tstep, d + it.second);
+    cudaStream_t st = S_.stream();
+    if (cudaMemcpyAsync(hstage_ + (size_t)slot * cap_, d, n * sizeof(double), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaEventRecord(slots_[slot].done, st) != cudaSuccess)
+        throw std::runtime_error("CUDA error queueing output copy");
+    slots_[slot].tstep = tstep;
+    slots_[slot].items = due;
+    slots_[slot].pending = true;
+    next_ = 1 - slot;
 }
 
 void OutputList::close() {
     if (closed_) return;
     closed_ = true;
+    flush(next_);       // the older slot first, then the newer
+    flush(1 - next_);
     for (Unit& u : units_) {
         if (u.tfile) std::fclose(u.tfile);
         if (u.data) std::fclose(u.data);
@@ -303,6 +355,10 @@ OutputList::~OutputList() {
         if (u.tfile) std::fclose(u.tfile);
         if (u.data) std::fclose(u.data);
     }
+    for (Slot& sl : slots_)
+        if (sl.done) cudaEventDestroy(sl.done);
+    if (dstage_) cudaFree(dstage_);
+    if (hstage_) cudaFreeHost(hstage_);
 }
 
 }  // namespace fdf

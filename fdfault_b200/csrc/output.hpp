@@ -7,7 +7,15 @@
 //   {datadir}{problem}_front_{n}_t.dat (+ _x/_y/_z, .m, .py) first times V >= threshold
 // Semantics follow src/outputunit.cpp:13-889 and src/front.cpp:17-359 for a
 // single process owning the whole grid.
+//
+// At an output step the due units' index windows are gathered on the device
+// (with the absolute-stress conversion of the read-back) into one staging
+// slot and copied to pinned host memory by one asynchronous copy on the
+// solver stream; the files are written when the slot is needed again two
+// output steps later, or at close, so the copies overlap the steps between.
 #pragma once
+
+#include <cuda_runtime.h>
 
 #include <cstdio>
 #include <string>
@@ -38,11 +46,24 @@ class OutputList {
         long long offset = 0;   // offset of the tangential component in a 2-component fault array
     };
     void open_unit(Unit& u);
+    void enqueue(Unit& u, int tstep, double* dst);   // gather u's window at this step into dst (device)
+    void flush(int slot);                             // wait for a slot's copy and write its files
     Solver& S_;
     std::vector<Unit> units_;
     bool needs_abs_ = false;
     bool closed_ = false;
-    std::vector<double> hbuf_;
+    // two staging slots (device + pinned host), each sized for every unit's window
+    struct Slot {
+        int tstep = -1;
+        std::vector<std::pair<int, size_t>> items;   // (unit, offset in the slot)
+        cudaEvent_t done = nullptr;
+        bool pending = false;
+    };
+    Slot slots_[2];
+    int next_ = 0;
+    size_t cap_ = 0;
+    double* dstage_ = nullptr;
+    double* hstage_ = nullptr;
 };
 
 }  // namespace fdf

@@ -1013,8 +1013,10 @@ void Solver::solve() {
         }
         out_->write(step_index_);
     }
+    // the status word is read every 16 steps (a device-side error stops the
+    // run within 16 steps of it), so output copies overlap the steps between
     while (step_index_ < nt_) {
-        step(1);
+        step(std::min(16, nt_ - step_index_));
         if (int st = check_status()) throw std::runtime_error("solver status " + std::to_string(st));
     }
     out_->close();
@@ -1329,6 +1331,11 @@ static double* fault_array(const IfaceDev& I, int which) {
         case 12: return I.tfront;
     }
     return nullptr;
+}
+
+double* Solver::fault_ptr(int iface, int which) const {
+    if (iface < 0 || iface >= (int)ifaces_.size()) return nullptr;
+    return fault_array(ifaces_[iface], which);
 }
 
 long long Solver::fault_count(int iface, int which) const {

@@ -53,6 +53,7 @@ class Solver {
     // volume component as the output list writes it at step tstep (absolute stress)
     void fetch_output_component(int comp, int tstep, double* out);
     void get_fault(int iface, int which, double* out);
+    double* fault_ptr(int iface, int which) const;   // device array of a fault quantity (or null)
     void set_fault(int iface, int which, const double* in);
     long long fault_count(int iface, int which) const;
 

@@ -8,6 +8,11 @@ reference sources (to build the binary); the fixtures it writes are what the
 tests read on machines without them.
 
     python tests/golden/make_golden.py [case ...]
+    python tests/golden/make_golden.py --files   # output_files.npz (below)
+
+``--files`` stores, for the cases in FILE_CASES, the bytes of every file the
+reference writes for its output units and fronts (data, time, coordinate and
+.m/.py metadata files) in tests/golden/output_files.npz, keyed "case/file".
 """
 
 import os
@@ -40,6 +45,26 @@ def read_outputs(prob, datadir):
     return out
 
 
+FILE_CASES = ["m2_sw", "p3_sw", "m2_curve"]
+
+
+def main_files():
+    if not os.path.exists(oracle.REF_BIN):
+        oracle.build()
+    arrays = {}
+    for name in FILE_CASES:
+        tmp = tempfile.mkdtemp(prefix="golden_files_")
+        prob = build_case(name, tmp)
+        infile = prob.write(os.path.join(tmp, prob.name + ".in"))
+        oracle.run_reference(infile, tmp)
+        for fn in sorted(os.listdir(tmp)):
+            if fn.startswith(prob.name + "_"):
+                with open(os.path.join(tmp, fn), "rb") as fh:
+                    arrays["%s/%s" % (name, fn)] = np.frombuffer(fh.read(), dtype=np.uint8)
+    np.savez_compressed(os.path.join(HERE, "output_files.npz"), **arrays)
+    print(len(arrays), "files", sum(a.size for a in arrays.values()), "bytes")
+
+
 def main(names):
     if not os.path.exists(oracle.REF_BIN):
         oracle.build()
@@ -54,4 +79,7 @@ def main(names):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:])
+    if sys.argv[1:] == ["--files"]:
+        main_files()
+    else:
+        main(sys.argv[1:])
