@@ -347,21 +347,45 @@ static long long mem_extent(MPI_Datatype t) {
     }
 }
 
+/* one contiguous piece of file I/O, repeated until every byte is moved */
+static int io_run(int fd, char *mp, long long len, long long off, int write_mode) {
+    while (len > 0) {
+        ssize_t n = write_mode ? pwrite(fd, mp, (size_t)len, (off_t)off) : pread(fd, mp, (size_t)len, (off_t)off);
+        if (n <= 0) return MPI_ERR_OTHER;
+        mp += n;
+        off += n;
+        len -= n;
+    }
+    return MPI_SUCCESS;
+}
+
+/* Elements are visited in the order the view and the memory type define;
+ * runs that are contiguous both in memory and in the file are moved by one
+ * system call each. */
 static int file_io(MPI_File fh, void *buf, int count, MPI_Datatype datatype, int write_mode) {
     int bsz = datatype->basic_size;
     if (bsz != fh->esize) die("etype/memory type size mismatch");
     long long per = mem_count(datatype), ext = mem_extent(datatype);
     char *base = (char *)buf;
+    char *run_mp = NULL;
+    long long run_off = 0, run_len = 0;
     for (int c = 0; c < count; c++) {
         for (long long e = 0; e < per; e++) {
             char *mp = base + ((long long)c * ext + mem_elem(datatype, e)) * bsz;
             long long off = view_offset(fh, fh->pos);
-            ssize_t n = write_mode ? pwrite(fh->fd, mp, (size_t)bsz, (off_t)off)
-                                   : pread(fh->fd, mp, (size_t)bsz, (off_t)off);
-            if (n != bsz) return MPI_ERR_OTHER;
+            if (run_len > 0 && mp == run_mp + run_len && off == run_off + run_len) {
+                run_len += bsz;
+            } else {
+                if (run_len > 0 && io_run(fh->fd, run_mp, run_len, run_off, write_mode) != MPI_SUCCESS)
+                    return MPI_ERR_OTHER;
+                run_mp = mp;
+                run_off = off;
+                run_len = bsz;
+            }
             fh->pos++;
         }
     }
+    if (run_len > 0 && io_run(fh->fd, run_mp, run_len, run_off, write_mode) != MPI_SUCCESS) return MPI_ERR_OTHER;
     return MPI_SUCCESS;
 }
 
