@@ -292,6 +292,10 @@ int fdf_bytes_per_node_stage(fdf_handle* h, long long* bytes) {
     return guarded(h, [&](fdf::Solver& s) { *bytes = s.bytes_per_node_stage(); });
 }
 
+int fdf_set_plastic_rule(fdf_handle* h, int rule) {
+    return guarded(h, [&](fdf::Solver& s) { s.set_plastic_rule(rule); });
+}
+
 int fdf_stz_set_start(fdf_handle* h, int mode) {
     return guarded(h, [&](fdf::Solver& s) { s.set_stz_start(mode); });
 }

@@ -8,7 +8,7 @@
 // the rationals in norm_weights() below.  The discrete energy of a block is
 //   E = sum_nodes  w_ijk J_ijk ( 1/2 rho |v|^2  +  1/2 sigma : S : sigma ),
 //   w_ijk = H_i H_j H_k dxi dxeta dzeta,
-// S the isotropic compliance (plane strain: sigma_zz = nu (sigma_xx + sigma_yy);
+// S the isotropic compliance of the node's material (plane strain: sigma_zz = nu (sigma_xx + sigma_yy);
 // antiplane: sigma_xz and sigma_yz only), J the Jacobian of the block's map.
 // Its rate under the semi-discrete operator L (volume terms, outer SATs and
 // interface conditions together) is
@@ -81,6 +81,12 @@ __global__ void __launch_bounds__(256) k_energy(EnergyArgs<T> a, BlockDev B, Nor
                                            : node_index(L, B.lo[0] + i, B.lo[1] + j, 0);
         double w = hw(W, i, n0) * hw(W, j, n1) * B.dx[0] * B.dx[1] * (double)a.J[id];
         if (L.ndim == 3) w *= hw(W, k, n2) * B.dx[2];
+        double rho = B.rho, lam = B.lam, g = B.g;
+        if (B.mat) {   // heterogeneous material
+            rho = B.mat[id];
+            lam = B.mat[B.matstride + id];
+            g = B.mat[2 * B.matstride + id];
+        }
         double v[3] = {0., 0., 0.}, rv[3] = {0., 0., 0.}, s[6] = {0., 0., 0., 0., 0., 0.}, rs[6] = {0., 0., 0., 0., 0., 0.};
         auto f = [&](int c) { return (double)a.F[c * cs + id]; };
         auto d = [&](int c) { return a.R ? (double)a.R[c * cs + id] : 0.; };
@@ -97,7 +103,7 @@ __global__ void __launch_bounds__(256) k_energy(EnergyArgs<T> a, BlockDev B, Nor
             v[0] = f(0), v[1] = f(1), rv[0] = d(0), rv[1] = d(1);
             s[0] = f(2), s[1] = f(3), s[3] = f(4);
             rs[0] = d(2), rs[1] = d(3), rs[3] = d(4);
-            const double nu = 0.5 * B.lam / (B.lam + B.g);
+            const double nu = 0.5 * lam / (lam + g);
             s[5] = nu * (s[0] + s[3]);
             rs[5] = nu * (rs[0] + rs[3]);
         } else {   // mode III: vz, sxz, syz
@@ -105,10 +111,10 @@ __global__ void __launch_bounds__(256) k_energy(EnergyArgs<T> a, BlockDev B, Nor
             s[2] = f(1), s[4] = f(2);
             rs[2] = d(1), rs[4] = d(2);
         }
-        const double kin = 0.5 * B.rho * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-        const double kr = B.rho * (v[0] * rv[0] + v[1] * rv[1] + v[2] * rv[2]);
+        const double kin = 0.5 * rho * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        const double kr = rho * (v[0] * rv[0] + v[1] * rv[1] + v[2] * rv[2]);
         double ws, wr;
-        strain_terms(B.lam, B.g, s, rs, &ws, &wr);
+        strain_terms(lam, g, s, rs, &ws, &wr);
         ek += w * kin;
         es += w * ws;
         er += w * (kr + wr);

@@ -43,6 +43,19 @@ struct BlockDev {
     const double* fnx[6][3];  // unit normals on the face, [n_a][n_b]
     const double* fdl[6];     // |grad xi|/(h0 dxi) on the face
     int fn1[6];               // second extent of the face arrays
+    // heterogeneous material (fields.cpp:582-711): rho, lambda, G per node at
+    // mat[c * matstride + node] (the whole grid, shared by all blocks; matstride
+    // is the layout's cstride), or null
+    const double* mat;
+    long long matstride;
+    // which nodes the plastic return map visits and with which bulk modulus.
+    // block::calc_plastic (block.cpp:442-589) declares `double k` and then an
+    // `int k` z-loop index, so its k = lambda + 2/3 G lands in the loop index:
+    // ptrunc 1 passes the modulus truncated to an integer; pvisit 0 every node,
+    // 1 only the block's first z node of each column, 2 the nodes pmask marks
+    // (the reference's z loop resumes at trunc(K) + 1)
+    int ptrunc, pvisit;
+    const unsigned char* pmask;
 };
 
 struct PertDev {

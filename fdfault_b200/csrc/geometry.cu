@@ -155,7 +155,7 @@ __global__ void k_face_normals(Layout L, int d, int at, int lo0, int n0, int lo1
 }
 
 __global__ void k_max_speed(Layout L, GeoBlock g, double cs, const double* __restrict__ M,
-                            unsigned long long* __restrict__ out) {
+                            const double* __restrict__ mat, unsigned long long* __restrict__ out) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     long long nn = (long long)g.n[0] * g.n[1] * g.n[2];
     double best = 0.;
@@ -164,6 +164,7 @@ __global__ void k_max_speed(Layout L, GeoBlock g, double cs, const double* __res
         int j = (int)((t / g.n[2]) % g.n[1]);
         int i = (int)(t / ((long long)g.n[2] * g.n[1]));
         long long id = nidx(L, g.lo[0] + i, g.lo[1] + j, g.lo[2] + k);
+        if (mat) cs = sqrt(mat[2 * L.cstride + id] / mat[id]);   // block.cpp:387-388
         for (int l = 0; l < L.ndim; l++) {
             double s = 0.;
             for (int m = 0; m < L.ndim; m++) {
@@ -232,10 +233,10 @@ void launch_face_normals(const Layout& L, int d, int at, int lo0, int n0, int lo
                                                                  nx[1], nx[2], dl, dl2, at2, h0dx2);
 }
 
-void launch_max_speed(const Layout& L, const GeoBlock& g, double cs, const double* M, unsigned long long* out,
-                      cudaStream_t s) {
+void launch_max_speed(const Layout& L, const GeoBlock& g, double cs, const double* M, const double* mat,
+                      unsigned long long* out, cudaStream_t s) {
     long long nn = (long long)g.n[0] * g.n[1] * g.n[2];
-    k_max_speed<<<nblk(nn, 256), 256, 0, s>>>(L, g, cs, M, out);
+    k_max_speed<<<nblk(nn, 256), 256, 0, s>>>(L, g, cs, M, mat, out);
 }
 
 template <typename T>

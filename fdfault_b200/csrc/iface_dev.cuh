@@ -603,7 +603,13 @@ __device__ __forceinline__ void interface_node(const IfaceArgs<T>& a, const Ifac
     load_abs(a, F, i2, b2);
     BF<double> br1 = rot_xy_nt(b1, nv, t1, t2), br2 = rot_xy_nt(b2, nv, t1, t2);
     BF<double> bs1 = br1, bs2 = br2;
-    const double zp1 = I.zp1, zs1 = I.zs1, zp2 = I.zp2, zs2 = I.zs2;
+    double zp1 = I.zp1, zs1 = I.zs1, zp2 = I.zp2, zs2 = I.zs2;
+    double cp1 = I.cp1, cs1 = I.cs1, cp2 = I.cp2, cs2 = I.cs2, gamma1 = I.gamma1, gamma2 = I.gamma2;
+    if (B1.mat) {   // heterogeneous material: both sides' nodes (interface.cpp:614-638)
+        const NodeMat m1 = node_material(B1.mat, B1.matstride, i1), m2 = node_material(B2.mat, B2.matstride, i2);
+        cp1 = m1.cp, cs1 = m1.cs, zp1 = m1.zp, zs1 = m1.zs, gamma1 = m1.gamma;
+        cp2 = m2.cp, cs2 = m2.cs, zp2 = m2.zp, zs2 = m2.zs, gamma2 = m2.gamma;
+    }
     // normal characteristic: locked solve (interface.cpp:1017-1028)
     double hs11 = (zp2 * (br1.s11 - zp1 * br1.v1) + zp1 * (br2.s11 + zp2 * br2.v1)) / (zp1 + zp2);
     double hv11 = (hs11 - br1.s11) / zp1 + br1.v1;
@@ -693,7 +699,6 @@ __device__ __forceinline__ void interface_node(const IfaceArgs<T>& a, const Ifac
     if (!isfinite(hs12) || !isfinite(hv12)) status |= FDF_ERR_NONFINITE;
     if (status) atomicOr(a.status, status);
     if (!no_sat) {
-        const double gamma1 = I.gamma1, gamma2 = I.gamma2;
         br1.v1 -= hv11;
         br1.v2 = 0.;
         br1.v3 = 0.;
@@ -714,8 +719,8 @@ __device__ __forceinline__ void interface_node(const IfaceArgs<T>& a, const Ifac
         br2.s23 = 0.;
         b1 = rot_nt_xy(br1, nv, t1, t2);
         b2 = rot_nt_xy(br2, nv, t1, t2);
-        sat_sub<T>(L, plastic, a.DF, i1, I.cp1 * h1, b1, true);
-        sat_sub<T>(L, plastic, a.DF, i2, I.cp2 * h2, b2, true);
+        sat_sub<T>(L, plastic, a.DF, i1, cp1 * h1, b1, true);
+        sat_sub<T>(L, plastic, a.DF, i2, cp2 * h2, b2, true);
         bs1.v1 = 0.;
         bs1.v2 -= hv12;
         bs1.v3 -= hv13;
@@ -736,8 +741,8 @@ __device__ __forceinline__ void interface_node(const IfaceArgs<T>& a, const Ifac
         bs2.s33 = 0.;
         b1 = rot_nt_xy(bs1, nv, t1, t2);
         b2 = rot_nt_xy(bs2, nv, t1, t2);
-        sat_sub<T>(L, plastic, a.DF, i1, I.cs1 * h1, b1, false);
-        sat_sub<T>(L, plastic, a.DF, i2, I.cs2 * h2, b2, false);
+        sat_sub<T>(L, plastic, a.DF, i1, cs1 * h1, b1, false);
+        sat_sub<T>(L, plastic, a.DF, i2, cs2 * h2, b2, false);
         if (fric) {
             // friction::calc_df and friction::update
             const double Bc = sa.B;

@@ -134,8 +134,10 @@ ProblemSpec read_problem(const std::string& infile) {
         P.matfile = s.str();
         P.plastic_tensor = s.integer() != 0;
     }
-    if (P.matfile != "none")
-        throw std::runtime_error("heterogeneous material files are not supported on this path");
+    if (P.matfile != "none" && P.ndim == 2 && P.mode == 3)
+        // the reference's time step reads a third material array that mode III
+        // does not have (block.cpp:387-388 with nmat = 2, fields.cpp:58-61)
+        throw std::runtime_error("heterogeneous material files are not supported for mode III");
     {
         Section s(infile, "[fdfault.operator]");
         P.cdiss = s.found() ? s.dbl() : 0.0;

@@ -21,8 +21,10 @@ void launch_metrics(const Layout& L, const GeoBlock& g, int order, const double*
 void launch_face_normals(const Layout& L, int d, int at, int lo0, int n0, int lo1, int n1, int flip, double h0dx,
                          const double* M, double* nx[3], double* dl, double* dl2, int at2, double h0dx2,
                          cudaStream_t s);
-void launch_max_speed(const Layout& L, const GeoBlock& g, double cs, const double* M, unsigned long long* out,
-                      cudaStream_t s);
+// largest cs |grad xi_l| / dxi_l over the block; cs per node from mat
+// (rho, lambda, G planes) when mat is not null
+void launch_max_speed(const Layout& L, const GeoBlock& g, double cs, const double* M, const double* mat,
+                      unsigned long long* out, cudaStream_t s);
 template <typename T>
 void launch_stress_roundtrip(const Layout& L, T* F, const double* S, const double s0[6], cudaStream_t s);
 void launch_to_float(const double* a, float* b, long long n, cudaStream_t s);

@@ -225,6 +225,7 @@ Solver::Solver(const std::string& infile, int precision, int device) : precision
     }
     status_ = static_cast<int*>(dalloc(sizeof(int)));
     setup_geometry();
+    setup_plastic_visits(setup_material());
     setup_boundaries();
     set_time_step();
     set_block_coefficients();
@@ -254,7 +255,7 @@ Solver::~Solver() {
     out_.reset();
     for (void* p : owned_) cudaFree(p);
     for (void* p : {F_[0], F_[1], DF_, FP_, M_, J_, (void*)M64_, (void*)J64_, (void*)X_, (void*)S_, (void*)ABS_,
-                    (void*)scratch_})
+                    (void*)scratch_, (void*)mat_, (void*)pmask_})
         if (p) cudaFree(p);
     for (auto g : graph_exec_)
         if (g) cudaGraphExecDestroy(g);
@@ -340,6 +341,118 @@ void Solver::setup_geometry() {
     if (check_status() & FDF_ERR_JACOBIAN) throw std::runtime_error("jacobian must be positive: grid is not smooth enough");
 }
 
+// heterogeneous material: fields::read_mat (src/fields.cpp:582-711). The file
+// holds rho, lambda and G over the whole grid (C order, FP64, one array after
+// the other); every value must be positive (fields.cpp:648). The planes stay
+// FP64 in both precisions and are shared by all blocks.
+std::vector<double> Solver::setup_material() {
+    if (P_.matfile == "none") return {};
+    const size_t n = (size_t)P_.nx[0] * P_.nx[1] * P_.nx[2];
+    const int nmat = 3;
+    std::vector<double> h = read_doubles(P_.matfile, (size_t)nmat * n, 0);
+    for (size_t q = 0; q < h.size(); q++)
+        if (!(h[q] > 0.) || !std::isfinite(h[q]))
+            throw std::runtime_error("material properties must be positive and finite (" + P_.matfile + ", value " +
+                                     std::to_string(q) + ")");
+    const size_t cs = (size_t)L_.cstride;
+    cuda_check(cudaMalloc(&mat_, cs * nmat * sizeof(double)), "cudaMalloc material");
+    cuda_check(cudaMemsetAsync(mat_, 0, cs * nmat * sizeof(double), stream_), "memset");
+    double* tmp = scratch(n);
+    for (int c = 0; c < nmat; c++) {
+        cuda_check(cudaMemcpyAsync(tmp, h.data() + c * n, n * sizeof(double), cudaMemcpyHostToDevice, stream_),
+                   "upload material");
+        launch_store_component<double>(L_, mat_, c, tmp, stream_);
+        cuda_check(cudaStreamSynchronize(stream_), "upload material");
+    }
+    for (auto& B : blocks_) {
+        B.mat = mat_;
+        B.matstride = L_.cstride;
+    }
+    return h;
+}
+
+// the nodes block::calc_plastic reaches (block.cpp:442-589).  Its z loop
+// index is also where it stores the bulk modulus K = lambda + 2/3 G, so after
+// the first node of a column it continues at trunc(K) + 1: in 2D that ends
+// the column's only node; in 3D the loop leaves the block after the first z
+// node when trunc(K) + 1 is past the block's last z node, visits the node
+// trunc(K) + 1 when it is inside the block (with a heterogeneous material a
+// chain of nodes), and never ends when a chain comes back to a node.
+void Solver::setup_plastic_visits(const std::vector<double>& mat) {
+    pvisit_ref_ = 0;
+    if (!P_.plastic() || P_.ndim != 3) {
+        apply_plastic_rule();
+        return;
+    }
+    const size_t n = (size_t)P_.nx[0] * P_.nx[1] * P_.nx[2];
+    const int ny = P_.nx[1], nz = P_.nx[2];
+    std::vector<long long> extra;   // nodes reached beyond the first of a column
+    for (size_t bi = 0; bi < blocks_.size() && plastic_stuck_.empty(); bi++) {
+        const BlockDev& B = blocks_[bi];
+        const BlockSpec& bs = P_.blocks[bi];
+        const int lo2 = B.lo[2], hi2 = B.lo[2] + B.n[2];
+        for (int i = B.lo[0]; i < B.lo[0] + B.n[0] && plastic_stuck_.empty(); i++)
+            for (int j = B.lo[1]; j < B.lo[1] + B.n[1] && plastic_stuck_.empty(); j++) {
+                int visits = 0;
+                for (int k = lo2; k < hi2;) {
+                    if (k < lo2 || ++visits > nz + 1) {
+                        plastic_stuck_ = k < lo2 ? "the reference's plastic update (block.cpp:451-524) reaches nodes "
+                                                   "outside their block for this problem"
+                                                 : "the reference's plastic update (block.cpp:451-524) does not "
+                                                   "terminate for this problem: its z loop index is overwritten by "
+                                                   "the bulk modulus lambda + 2/3 G";
+                        break;
+                    }
+                    const size_t q = ((size_t)i * ny + j) * nz + k;
+                    const double K = mat.empty() ? bs.lam + 2. / 3. * bs.g : mat[n + q] + 2. / 3. * mat[2 * n + q];
+                    if (!(K < 2147483647.)) {
+                        plastic_stuck_ = "the bulk modulus lambda + 2/3 G does not fit the reference's int loop index";
+                        break;
+                    }
+                    if (k != lo2) extra.push_back((long long)i * L_.s0 + (long long)j * L_.s1 + k);
+                    k = (int)K + 1;
+                }
+            }
+    }
+    pvisit_ref_ = extra.empty() ? 1 : 2;
+    if (pvisit_ref_ == 2 && plastic_stuck_.empty()) {
+        std::vector<unsigned char> m((size_t)L_.cstride, 0);
+        for (const auto& B : blocks_)
+            for (int i = B.lo[0]; i < B.lo[0] + B.n[0]; i++)
+                for (int j = B.lo[1]; j < B.lo[1] + B.n[1]; j++)
+                    m[(size_t)i * L_.s0 + (size_t)j * L_.s1 + B.lo[2]] = 1;
+        for (long long q : extra) m[(size_t)q] = 1;
+        cuda_check(cudaMalloc(&pmask_, m.size()), "cudaMalloc plastic mask");
+        cuda_check(cudaMemcpy(pmask_, m.data(), m.size(), cudaMemcpyHostToDevice), "upload plastic mask");
+    }
+    apply_plastic_rule();
+}
+
+void Solver::apply_plastic_rule() {
+    for (auto& B : blocks_) {
+        B.ptrunc = plastic_rule_ == 0 ? 1 : 0;
+        B.pvisit = plastic_rule_ == 0 ? pvisit_ref_ : 0;
+        B.pmask = pmask_;
+    }
+}
+
+void Solver::check_plastic_rule() const {
+    if (P_.plastic() && plastic_rule_ == 0 && !plastic_stuck_.empty())
+        throw std::runtime_error(plastic_stuck_ + "; select the every-node rule (fdf_set_plastic_rule) to step it");
+}
+
+void Solver::set_plastic_rule(int rule) {
+    if (rule != 0 && rule != 1) throw std::invalid_argument("plastic rule must be 0 (reference) or 1 (every node)");
+    synchronize();
+    plastic_rule_ = rule;
+    apply_plastic_rule();
+    cuda_check(cudaMemcpyAsync(blocks_dev_, blocks_.data(), blocks_.size() * sizeof(BlockDev), cudaMemcpyHostToDevice,
+                               stream_),
+               "block table");
+    cuda_check(cudaStreamSynchronize(stream_), "block table");
+    graph_dirty_ = true;
+}
+
 // boundary::boundary + allocate_normals: src/boundary.cpp:15-240
 void Solver::setup_boundaries() {
     const int ndim = P_.ndim;
@@ -400,7 +513,7 @@ void Solver::set_time_step() {
             g.n[d] = B.n[d];
             g.dx[d] = B.dx[d];
         }
-        launch_max_speed(L_, g, B.cs, M64_, dmax, stream_);
+        launch_max_speed(L_, g, B.cs, M64_, mat_, dmax, stream_);
     }
     unsigned long long bits = 0;
     cuda_check(cudaMemcpyAsync(&bits, dmax, sizeof(bits), cudaMemcpyDeviceToHost, stream_), "min dx");
@@ -775,7 +888,9 @@ void Solver::profile_read(int kernel, double* total_ms, long long* launches) {
 }
 
 int Solver::volume_kernel_active() const {
-    if (vkernel_ == 0 || precision_ != 1) return 0;
+    // the marching kernels hold one material per block: heterogeneous
+    // material runs the reference-order kernel
+    if (vkernel_ == 0 || precision_ != 1 || mat_) return 0;
     if (L_.ndim == 2) {   // tiled 2D kernel (elastic, no dissipation; kinds 1 and 3) or none
         if ((vkernel_ != 1 && vkernel_ != 3) || P_.plastic() || P_.cdiss > 0.) return 0;
         for (auto& B : blocks_)
@@ -904,6 +1019,7 @@ void Solver::stage_impl(double dt, int stage, double t, bool for_step) {
 
 void Solver::do_rk_stage(double dt, int stage, double t) {
     if (stage < 0 || stage >= nstages_) throw std::runtime_error("stage out of range");
+    check_plastic_rule();
     if (precision_ == 0)
         stage_impl<double>(dt, stage, t, false);
     else
@@ -912,6 +1028,7 @@ void Solver::do_rk_stage(double dt, int stage, double t) {
 }
 
 void Solver::step(int nsteps) {
+    check_plastic_rule();
     // whole pairs of steps replay the captured graph when nothing on the host
     // has to happen between steps (no output units, no per-launch profiling)
     if (graphs_ && !out_ && !profile_ && nsteps >= 2) {

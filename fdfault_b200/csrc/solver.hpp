@@ -63,6 +63,8 @@ class Solver {
     // warm start from each node's previous root, 3 midpoint with the exact
     // derivative (1 is the learned start, set_stz_learned)
     void set_stz_start(int mode);
+    void set_plastic_rule(int rule);
+    int plastic_rule() const { return plastic_rule_; }
     void set_stz_counting(bool on);
     void read_stz_counts(long long out[3], bool reset);
     void stz_collect(long long capacity);            // 0 stops collecting and frees the buffer
@@ -128,6 +130,10 @@ class Solver {
     template <typename T>
     void init_fields();
     void setup_geometry();
+    std::vector<double> setup_material();
+    void setup_plastic_visits(const std::vector<double>& mat);
+    void apply_plastic_rule();
+    void check_plastic_rule() const;
     void setup_boundaries();
     void setup_interfaces();
     void set_time_step();
@@ -163,6 +169,13 @@ class Solver {
     double* J64_ = nullptr;
     double* X_ = nullptr;
     double* S_ = nullptr;
+    double* mat_ = nullptr;   // heterogeneous material planes rho, lambda, G (FP64) or null
+    // plastic return map: 0 the reference's loop (truncated modulus, the nodes
+    // its z loop reaches), 1 every node with the exact modulus
+    int plastic_rule_ = 0;
+    int pvisit_ref_ = 0;                  // pvisit of the reference rule (0, 1 or 2)
+    unsigned char* pmask_ = nullptr;      // nodes the reference's z loop reaches (pvisit 2)
+    std::string plastic_stuck_;           // why the reference's loop would not finish, or empty
     double* ABS_ = nullptr;
     int* status_ = nullptr;
     double* scratch_ = nullptr;

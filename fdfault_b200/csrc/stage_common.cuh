@@ -62,16 +62,42 @@ __device__ __forceinline__ BF<T> rot_nt_xy(const BF<T>& b, const T nn[3], const 
     return o;
 }
 
+// wave speeds, impedances and gamma = 1 - 2 (cs/cp)^2 of one node of a
+// heterogeneous material (planes rho, lambda, G at stride st), in the
+// reference's expressions (boundary.cpp:303-314, interface.cpp:614-638)
+struct NodeMat {
+    double cp, cs, zp, zs, gamma;
+};
+__device__ __forceinline__ NodeMat node_material(const double* mat, long long st, long long id) {
+    NodeMat m;
+    const double rho = mat[id], lm = mat[st + id], gg = mat[2 * st + id];
+    m.cp = sqrt((lm + 2. * gg) / rho);
+    m.cs = sqrt(gg / rho);
+    m.zp = rho * m.cp;
+    m.zs = rho * m.cs;
+    m.gamma = 1. - 2. * ((m.cs / m.cp) * (m.cs / m.cp));
+    return m;
+}
+
 // Outer-boundary SAT on face `face` of block b for the node at (a,b) in the
 // face arrays; f holds the node's stage-start fields, df its rate register.
 template <typename T, int NDIM, int MODE>
 __device__ __forceinline__ void boundary_sat(const BlockDev& B, int face, int fa, int fb, T dt, const T* f, T* df,
-                                             bool plastic) {
+                                             bool plastic, long long id = -1) {
     const long long ij = (long long)fa * B.fn1[face] + fb;
     T nn[3] = {T(0.), T(0.), T(0.)}, t1[3], t2[3];
     for (int l = 0; l < NDIM; l++) nn[l] = (T)B.fnx[face][l][ij];
     const T h = dt * (T)B.fdl[face][ij];
-    const T cp = (T)B.cp, cs = (T)B.cs, zp = (T)B.zp, zs = (T)B.zs, gamma = (T)B.gamma, r = (T)B.r[face];
+    T cp = (T)B.cp, cs = (T)B.cs, zp = (T)B.zp, zs = (T)B.zs, gamma = (T)B.gamma;
+    const T r = (T)B.r[face];
+    if (B.mat && id >= 0) {   // per-node material; id is the node
+        const NodeMat m = node_material(B.mat, B.matstride, id);
+        cp = (T)m.cp;
+        cs = (T)m.cs;
+        zp = (T)m.zp;
+        zs = (T)m.zs;
+        gamma = (T)m.gamma;
+    }
     if (fabs(nn[0]) > fabs(nn[1]) && fabs(nn[0]) > fabs(nn[2])) {
         t1[2] = T(0.);
         t1[1] = nn[0] / sqrt(nn[0] * nn[0] + nn[1] * nn[1]);
@@ -249,8 +275,21 @@ __device__ __forceinline__ void finish_node(const Layout& L, const BlockDev& B, 
             in.epyz = (double)FP[6 * L.cstride + id]; in.epzz = (double)FP[7 * L.cstride + id];
         }
         (void)o;
-        const double k = B.lam + 2. / 3. * B.g;
-        Plastp out = plastic_flow(B, sa.dt, in, k, B.g);
+        double lm = B.lam, gg = B.g;
+        if (B.mat) {   // block.cpp:519-521
+            lm = B.mat[L.cstride + id];
+            gg = B.mat[2 * L.cstride + id];
+        }
+        double k = lm + 2. / 3. * gg;
+        if (B.ptrunc) k = (double)(int)k;   // the int loop index holds it (block.cpp:519-524)
+        bool visit = true;
+        if (B.pvisit == 1)
+            visit = (int)(id % L.s1) == B.lo[2];
+        else if (B.pvisit == 2)
+            visit = B.pmask[id] != 0;
+        // a node the loop skips keeps its stress (through the absolute-stress
+        // round trip below) and its plastic fields
+        Plastp out = visit ? plastic_flow(B, sa.dt, in, k, gg) : in;
         if (L.ndim == 3) {
             sv[0] = out.sxx; sv[1] = out.sxy; sv[2] = out.sxz; sv[3] = out.syy; sv[4] = out.syz; sv[5] = out.szz;
         } else if (L.mode == 2) {
@@ -258,12 +297,14 @@ __device__ __forceinline__ void finish_node(const Layout& L, const BlockDev& B, 
         } else {
             sv[0] = out.sxz; sv[1] = out.syz;
         }
-        FP[0 * L.cstride + id] = (T)out.lambda;
-        FP[1 * L.cstride + id] = (T)out.gammap;
-        if (plastic_tensor) {
-            FP[2 * L.cstride + id] = (T)out.epxx; FP[3 * L.cstride + id] = (T)out.epxy;
-            FP[4 * L.cstride + id] = (T)out.epxz; FP[5 * L.cstride + id] = (T)out.epyy;
-            FP[6 * L.cstride + id] = (T)out.epyz; FP[7 * L.cstride + id] = (T)out.epzz;
+        if (visit) {
+            FP[0 * L.cstride + id] = (T)out.lambda;
+            FP[1 * L.cstride + id] = (T)out.gammap;
+            if (plastic_tensor) {
+                FP[2 * L.cstride + id] = (T)out.epxx; FP[3 * L.cstride + id] = (T)out.epxy;
+                FP[4 * L.cstride + id] = (T)out.epxz; FP[5 * L.cstride + id] = (T)out.epyy;
+                FP[6 * L.cstride + id] = (T)out.epyz; FP[7 * L.cstride + id] = (T)out.epzz;
+            }
         }
         for (int c = 0; c < L.ns; c++) {
             if (sizeof(T) == 8) {

@@ -43,7 +43,14 @@ __device__ __forceinline__ void volume_node(const VolumeArgs<T>& a, const BlockD
     const T cdiss = (T)a.cdiss;
     const T jc = J[id];
     for (int d = 0; d < NDIM; d++) {
-        const T invrho = (T)B.coef[d][0], g2lam = (T)B.coef[d][1], g = (T)B.coef[d][2], lambda = (T)B.coef[d][3];
+        T invrho = (T)B.coef[d][0], g2lam = (T)B.coef[d][1], g = (T)B.coef[d][2], lambda = (T)B.coef[d][3];
+        if (B.mat) {   // per-node material (block.cpp:1061-1065 and the other passes)
+            const double rho = B.mat[id], lm = B.mat[cs + id], gg = B.mat[2 * cs + id];
+            invrho = (T)(sa.dt / rho / B.dx[d]);
+            g2lam = (T)(sa.dt * (2. * gg + lm) / B.dx[d]);
+            g = (T)(sa.dt * gg / B.dx[d]);
+            lambda = (T)(sa.dt * lm / B.dx[d]);
+        }
         const T invjac = invrho / jc;
         const int pp = p[d], n = B.n[d];
         int row, ntap;
@@ -120,7 +127,21 @@ __device__ __forceinline__ void volume_node(const VolumeArgs<T>& a, const BlockD
             }
         }
     }
-    if (NDIM == 2 && MODE == 2 && plastic) df[5] = (T)B.nu * (df[2] + df[4]);
+    if (NDIM == 2 && MODE == 2 && plastic) {
+        T nu = (T)B.nu;
+        if (B.mat) {
+            // block.cpp:1289-1291 reads lambda at the node and, as its second
+            // term, the material array one x row further on (mat[nxd[1] + index]):
+            // rho of node (i+1, j), or past the last row lambda of (0, j)
+            const int gi = B.lo[0] + p[0], gj = B.lo[1] + p[1], ny = L.nx[1];
+            const long long q = (long long)gi * ny + gj + ny, nxy = (long long)L.nx[0] * ny;
+            const long long qc = q / nxy, qr = q % nxy;
+            const double other = B.mat[qc * cs + node_index(L, (int)(qr / ny), (int)(qr % ny), 0)];
+            const double lm = B.mat[cs + id];
+            nu = (T)(0.5 * lm / (lm + other));
+        }
+        df[5] = nu * (df[2] + df[4]);
+    }
     // outer-face SATs (block::set_boundaries: faces in order)
     bool defer = false;
     bool onface = false;
@@ -145,7 +166,7 @@ __device__ __forceinline__ void volume_node(const VolumeArgs<T>& a, const BlockD
         T fv[9];
 #pragma unroll
         for (int q = 0; q < NF; q++) fv[q] = F[q * cs + id];
-        boundary_sat<T, NDIM, MODE>(B, f, fa, fb, (T)sa.dt, fv, df, plastic);
+        boundary_sat<T, NDIM, MODE>(B, f, fa, fb, (T)sa.dt, fv, df, plastic, id);
     }
     (void)onface;
     for (int q = 0; q < nfd; q++) a.DF[q * cs + id] = df[q];

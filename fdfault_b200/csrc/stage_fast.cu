@@ -561,6 +561,7 @@ void launch_plastic(const VolumeArgs<float>& a, const BlockDev& b, const StageAr
 }  // namespace
 
 bool fast3d_supported(const Layout& L, const BlockDev& b, int order) {
+    if (b.mat) return false;   // one material per block
     if (L.ndim != 3 || L.nfields != 9) return false;
     if (order < 2 || order > 4) return false;
     if (b.n[1] < TJ || b.n[2] < TK) return false;

@@ -464,6 +464,7 @@ void launch_ens2(int grid, const EnsMember* mem, const Ens2dItem* items, int nit
 }  // namespace
 
 bool fast2d_supported(const Layout& L, const BlockDev& b, int order) {
+    if (b.mat) return false;   // one material per block
     if (L.ndim != 2) return false;
     if (!((L.mode == 2 && L.nfields == 5) || (L.mode == 3 && L.nfields == 3))) return false;   // elastic only
     if (order < 2 || order > 4) return false;

@@ -642,6 +642,7 @@ RegMapsHost* make_reg_maps(const Layout& L, const float* F0, const float* F1, co
 void free_reg_maps(RegMapsHost* h) { delete h; }
 
 bool reg3d_supported(const Layout& L, const BlockDev& b, int order) {
+    if (b.mat) return false;   // one material per block
     if (L.ndim != 3 || L.nfields != 9) return false;
     if (order < 2 || order > 4) return false;
     if (b.n[1] < TJ || b.n[2] < TK) return false;

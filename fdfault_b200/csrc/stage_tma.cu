@@ -533,6 +533,7 @@ StagedMapsHost* make_staged_maps(const Layout& L, const float* F0, const float* 
 void free_staged_maps(StagedMapsHost* h) { delete h; }
 
 bool staged3d_supported(const Layout& L, const BlockDev& b, int order) {
+    if (b.mat) return false;   // one material per block
     if (L.ndim != 3 || L.nfields != 9) return false;
     if (order < 2 || order > 4) return false;
     if (b.n[1] < TJ || b.n[2] < TK) return false;

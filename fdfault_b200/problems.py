@@ -265,6 +265,39 @@ def lognormal_field(n0: int, n1: int, h: float, mean: float, sd: float, corr: fl
     return np.exp(mu_ln + np.sqrt(s2) * g)
 
 
+def write_material(path: str, rho: np.ndarray, lam: np.ndarray, g: np.ndarray) -> str:
+    """Heterogeneous material file (fields.cpp:582-711): density, Lame's first
+    parameter and shear modulus over the whole grid, each an (nx, ny, nz) array
+    in C order (nz = 1 in 2D), written one after the other as little-endian
+    FP64.  Every value must be positive.  Set the problem's ``matfile`` to the
+    returned path; the blocks' own (rho, lam, g) are then not used by the
+    time stepping."""
+    arrs = [np.asarray(a, dtype="<f8") for a in (rho, lam, g)]
+    if not all(a.shape == arrs[0].shape for a in arrs):
+        raise ValueError("material arrays differ in shape")
+    if not all(np.all(a > 0.) and np.all(np.isfinite(a)) for a in arrs):
+        raise ValueError("material properties must be positive and finite")
+    np.concatenate([a.reshape(-1) for a in arrs]).tofile(path)
+    return path
+
+
+def layered_material(prob: "Problem", path: str, seed: int, contrast: float = 0.2,
+                     noise: float = 0.05) -> str:
+    """Write a seeded heterogeneous material for ``prob`` and point its
+    ``matfile`` at it: each of rho, lambda and G is the first block's value
+    times (1 + contrast * (y - 1/2) + noise * U[-1, 1]) with y the node's
+    relative position across the grid in y, so a fault normal to y sees a
+    different material on each side and every node its own."""
+    nx, ny, nz = prob.nx
+    b = next(iter(prob.blocks.values()))
+    rng = np.random.default_rng(seed)
+    y = (np.arange(ny) / max(ny - 1, 1))[None, :, None]
+    arrs = [base * (1. + contrast * (y - 0.5) + noise * rng.uniform(-1., 1., (nx, ny, nz)))
+            for base in (b.rho, b.lam, b.g)]
+    prob.matfile = write_material(path, *arrs)
+    return path
+
+
 # CFL number of the full-size 3D workloads (two blocks of 401 x 201 x 201 at
 # h = 0.1 km, RK3).  At CFL 0.3 and 0.25 both precisions grow without bound at
 # the corners where the fault meets the absorbing x and z- faces after about

@@ -70,6 +70,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fdf_use_fast_kernel.argtypes = [ctypes.c_void_p, c_int, P(c_int)]
     L.fdf_set_volume_kernel.argtypes = [ctypes.c_void_p, c_int, P(c_int)]
     L.fdf_set_wait_limit.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
+    L.fdf_set_plastic_rule.argtypes = [ctypes.c_void_p, c_int]
     L.fdf_energy.argtypes = [ctypes.c_void_p, c_int, P(ctypes.c_double)]
     L.fdf_use_graphs.argtypes = [ctypes.c_void_p, c_int]
     L.fdf_bytes_per_node_stage.argtypes = [ctypes.c_void_p, P(c_ll)]
@@ -299,6 +300,15 @@ class Problem:
         self._check(self._L.fdf_energy(self._h, int(rate), out))
         return {"kinetic": out[0], "strain": out[1], "total": out[0] + out[1], "rate": out[2],
                 "rate_scale": out[3], "friction_power": out[4]}
+
+    PLASTIC_REFERENCE, PLASTIC_EVERY_NODE = 0, 1
+
+    def set_plastic_rule(self, rule: int) -> None:
+        """Return-map rule of plastic problems: 0 the reference's loop
+        (block.cpp:442-589; trunc(lambda + 2/3 G) as bulk modulus, in 3D the
+        first z node of each block column), 1 every node with the exact
+        modulus."""
+        self._check(self._L.fdf_set_plastic_rule(self._h, rule))
 
     def set_wait_limit(self, polls: int) -> None:
         """Polls of each bounded wait for staged data in volume kernels 2 and 3

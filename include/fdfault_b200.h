@@ -165,6 +165,23 @@ int fdf_set_volume_kernel(fdf_handle* h, int kind, int* active);
  * counterpart: the reference has no device waits. */
 int fdf_set_wait_limit(fdf_handle* h, long long polls);
 
+/* Nodes and bulk modulus of the Drucker-Prager return map (plastic problems).
+ * Rule 0, the default, is the reference's block::calc_plastic
+ * (src/block.cpp:442-589) as it runs: the function declares `double k` and
+ * then an `int k` z-loop index, so the bulk modulus K = lambda + 2/3 G it
+ * computes lands in the loop index.  The return map therefore gets trunc(K),
+ * and the z loop continues at trunc(K) + 1: every node in 2D, and in 3D the
+ * first z node of each column of a block (more with a heterogeneous material
+ * whose trunc(K) + 1 falls inside the block).  Where that loop would never
+ * end (3D blocks reaching z index trunc(K) + 1, e.g. nz > 54 for the usual
+ * lambda = G = 32.04) stepping under rule 0 fails with FDF_ERR_SOLVER and a
+ * message naming the loop.  Rule 1 applies the return map at every node with
+ * the exact K, the evident intent of that code; it has no reference result to
+ * match.  Changing the rule drops captured step graphs. */
+#define FDF_PLASTIC_REFERENCE 0
+#define FDF_PLASTIC_EVERY_NODE 1
+int fdf_set_plastic_rule(fdf_handle* h, int rule);
+
 /* FP64 energy diagnostics of an elastic problem, accumulated on the device
  * whatever the field precision, in the diagonal norm H of the SBP operator
  * (H D + D^T H = diag(-1, 0, ..., 0, 1); its first entry is the reference's

@@ -102,6 +102,8 @@ struct orc_problem {
     int nxyz, nxd[3];
     double *f, *df, *x, *metric, *jac, *s;
     int hetstress;
+    int hetmat;   /* material file: rho, lambda, G per node (fields.cpp:582-711) */
+    double *mat;
     double cdiss;
     int dissipation;
     block_t *blocks;
@@ -545,6 +547,23 @@ static int set_grid(orc_problem *p, block_t *b) {
 static double mat_cs(const block_t *b) { return sqrt(b->g / b->rho); }
 static double mat_cp(const block_t *b) { return sqrt((b->lam + 2. * b->g) / b->rho); }
 
+/* wave speeds, impedances and gamma of one node of a heterogeneous material:
+   boundary.cpp:303-314 and interface.cpp:614-638 (pow(x, 2) is x * x) */
+typedef struct {
+    double cp, cs, zp, zs, gamma;
+} nodemat_t;
+static nodemat_t node_mat(const orc_problem *p, long id) {
+    const long n = p->nxd[0];
+    const double rho = p->mat[id], lam = p->mat[n + id], g = p->mat[2 * n + id];
+    nodemat_t m;
+    m.cp = sqrt((lam + 2. * g) / rho);
+    m.cs = sqrt(g / rho);
+    m.zp = rho * m.cp;
+    m.zs = rho * m.cs;
+    m.gamma = 1. - 2. * ((m.cs / m.cp) * (m.cs / m.cp));
+    return m;
+}
+
 /* outer boundary set-up: src/boundary.cpp:15-240 */
 static void bound_init(orc_problem *p, block_t *b, int loc) {
     bound_t *bd = &b->bound[loc];
@@ -710,7 +729,15 @@ static void calc_df(orc_problem *p, block_t *b, double dt) {
                         step = -stride;
                         sg = -1.;
                     }
-                    const double invjac = invrho / J[i1];
+                    double ir = invrho, gl = g2lam, gg = g, la = lambda;
+                    if (p->hetmat) { /* per node (block.cpp:1061-1065 and the other passes) */
+                        const double rh = p->mat[i1], lm = p->mat[n0 + i1], gm = p->mat[2 * n0 + i1];
+                        ir = dt / rh / b->dx[d];
+                        gl = dt * (2. * gm + lm) / b->dx[d];
+                        gg = dt * gm / b->dx[d];
+                        la = dt * lm / b->dx[d];
+                    }
+                    const double invjac = ir / J[i1];
                     const double *cf = p->fdc[index3];
                     const double *dc = p->dsc[index3];
                     for (int n = 0; n < ntap; n++) {
@@ -724,28 +751,28 @@ static void calc_df(orc_problem *p, block_t *b, double dt) {
                             t[0] = (invjac * c * J[i2] * (ma * F[3 * n0 + i2] + mb * F[4 * n0 + i2] + mcc * F[5 * n0 + i2]));
                             t[1] = (invjac * c * J[i2] * (ma * F[4 * n0 + i2] + mb * F[6 * n0 + i2] + mcc * F[7 * n0 + i2]));
                             t[2] = (invjac * c * J[i2] * (ma * F[5 * n0 + i2] + mb * F[7 * n0 + i2] + mcc * F[8 * n0 + i2]));
-                            t[3] = c * (g2lam * ca * F[i2] + lambda * (cb * F[n0 + i2] + cc * F[2 * n0 + i2]));
-                            t[4] = c * g * (ca * F[n0 + i2] + cb * F[i2]);
-                            t[5] = c * g * (ca * F[2 * n0 + i2] + cc * F[i2]);
-                            t[6] = c * (g2lam * cb * F[n0 + i2] + lambda * (ca * F[i2] + cc * F[2 * n0 + i2]));
-                            t[7] = c * g * (cb * F[2 * n0 + i2] + cc * F[n0 + i2]);
-                            t[8] = c * (g2lam * cc * F[2 * n0 + i2] + lambda * (ca * F[i2] + cb * F[n0 + i2]));
+                            t[3] = c * (gl * ca * F[i2] + la * (cb * F[n0 + i2] + cc * F[2 * n0 + i2]));
+                            t[4] = c * gg * (ca * F[n0 + i2] + cb * F[i2]);
+                            t[5] = c * gg * (ca * F[2 * n0 + i2] + cc * F[i2]);
+                            t[6] = c * (gl * cb * F[n0 + i2] + la * (ca * F[i2] + cc * F[2 * n0 + i2]));
+                            t[7] = c * gg * (cb * F[2 * n0 + i2] + cc * F[n0 + i2]);
+                            t[8] = c * (gl * cc * F[2 * n0 + i2] + la * (ca * F[i2] + cb * F[n0 + i2]));
                         } else if (mode == 2) {
                             const double *m2 = M + (long)(d * ndim) * n0;
                             const double ma = m2[i2], mb = m2[n0 + i2];
                             const double ca = m2[i1], cb = m2[n0 + i1];
                             t[0] = (invjac * c * J[i2] * (ma * F[2 * n0 + i2] + mb * F[3 * n0 + i2]));
                             t[1] = (invjac * c * J[i2] * (ma * F[3 * n0 + i2] + mb * F[4 * n0 + i2]));
-                            t[2] = c * (g2lam * ca * F[i2] + lambda * cb * F[n0 + i2]);
-                            t[3] = g * c * (ca * F[n0 + i2] + cb * F[i2]);
-                            t[4] = c * (g2lam * cb * F[n0 + i2] + lambda * ca * F[i2]);
+                            t[2] = c * (gl * ca * F[i2] + la * cb * F[n0 + i2]);
+                            t[3] = gg * c * (ca * F[n0 + i2] + cb * F[i2]);
+                            t[4] = c * (gl * cb * F[n0 + i2] + la * ca * F[i2]);
                         } else {
                             const double *m2 = M + (long)(d * ndim) * n0;
                             const double ma = m2[i2], mb = m2[n0 + i2];
                             const double ca = m2[i1], cb = m2[n0 + i1];
                             t[0] = invjac * c * J[i2] * (ma * F[n0 + i2] + mb * F[2 * n0 + i2]);
-                            t[1] = g * ca * c * F[i2];
-                            t[2] = g * cb * c * F[i2];
+                            t[1] = gg * ca * c * F[i2];
+                            t[2] = gg * cb * c * F[i2];
                         }
                         for (int q = 0; q < nf; q++) {
                             if (sg > 0.)
@@ -766,6 +793,10 @@ static void calc_df(orc_problem *p, block_t *b, double dt) {
         for (int i = b->mlb[0]; i < b->prb[0]; i++)
             for (int j = b->mlb[1]; j < b->prb[1]; j++) {
                 long id = (long)i * nxd[1] + j;
+                /* the second term reads the material array one x row on
+                   (mat[nxd[1] + index], block.cpp:1289-1291): rho of (i+1, j),
+                   past the last row lambda of (0, j) */
+                if (p->hetmat) nu = 0.5 * p->mat[n0 + id] / (p->mat[n0 + id] + p->mat[nxd[1] + id]);
                 DF[5 * n0 + id] = nu * (DF[2 * n0 + id] + DF[4 * n0 + id]);
             }
     }
@@ -779,7 +810,7 @@ static void apply_bound(orc_problem *p, block_t *b, bound_t *bd, double dt) {
     const int *nxd = p->nxd;
     double *F = p->f, *DF = p->df;
     double nn[3] = {0., 0., 0.}, t1[3], t2[3], h = 0.;
-    const double cp = bd->cp, cs = bd->cs, zp = bd->zp, zs = bd->zs, gamma = bd->gamma, r = bd->r;
+    const double r = bd->r;
     (void)b;
     for (int i = bd->mlb[0]; i < bd->prb[0]; i++)
         for (int j = bd->mlb[1]; j < bd->prb[1]; j++)
@@ -794,6 +825,11 @@ static void apply_bound(orc_problem *p, block_t *b, bound_t *bd, double dt) {
                 for (int l = 0; l < ndim; l++) {
                     nn[l] = bd->nx[l][ij];
                     h = dt * bd->dl[ij];
+                }
+                double cp = bd->cp, cs = bd->cs, zp = bd->zp, zs = bd->zs, gamma = bd->gamma;
+                if (p->hetmat) {
+                    const nodemat_t m = node_mat(p, id);
+                    cp = m.cp; cs = m.cs; zp = m.zp; zs = m.zs; gamma = m.gamma;
                 }
                 if (fabs(nn[0]) > fabs(nn[1]) && fabs(nn[0]) > fabs(nn[2])) {
                     t1[2] = 0.;
@@ -1208,9 +1244,6 @@ static int iface_apply(orc_problem *p, iface_t *f, double dt, double t, int no_s
     double *F = p->f, *DF = p->df, *S = p->s;
     const double *s0 = p->s0;
     double nn[3] = {0., 0., 0.}, t1[3], t2[3];
-    const double cp1 = f->cp1, cs1 = f->cs1, zp1 = f->zp1, zs1 = f->zs1;
-    const double cp2 = f->cp2, cs2 = f->cs2, zp2 = f->zp2, zs2 = f->zs2;
-    const double gamma1 = f->gamma1, gamma2 = f->gamma2;
     for (int i = f->mlb[0]; i < f->prb[0]; i++)
         for (int j = f->mlb[1]; j < f->prb[1]; j++)
             for (int k = f->mlb[2]; k < f->prb[2]; k++) {
@@ -1223,6 +1256,14 @@ static int iface_apply(orc_problem *p, iface_t *f, double dt, double t, int no_s
                     default: ii = i - f->mlb[0]; jj = j - f->mlb[1];
                 }
                 long ij = (long)ii * f->n[1] + jj;
+                double cp1 = f->cp1, cs1 = f->cs1, zp1 = f->zp1, zs1 = f->zs1;
+                double cp2 = f->cp2, cs2 = f->cs2, zp2 = f->zp2, zs2 = f->zs2;
+                double gamma1 = f->gamma1, gamma2 = f->gamma2;
+                if (p->hetmat) {
+                    const nodemat_t m1 = node_mat(p, i1), m2 = node_mat(p, i2);
+                    cp1 = m1.cp; cs1 = m1.cs; zp1 = m1.zp; zs1 = m1.zs; gamma1 = m1.gamma;
+                    cp2 = m2.cp; cs2 = m2.cs; zp2 = m2.zp; zs2 = m2.zs; gamma2 = m2.gamma;
+                }
                 double h1 = dt * f->dl1[ij], h2 = dt * f->dl2[ij];
                 for (int l = 0; l < ndim; l++) nn[l] = f->nx[l][ij];
                 switch (f->direction) {
@@ -1435,17 +1476,42 @@ static plastp plastic_flow(const block_t *b, double dt, plastp in, double k, dou
     return out;
 }
 
-static void calc_plastic(orc_problem *p, block_t *b, double dt) {
+/* block::calc_plastic, src/block.cpp:442-589.  Its loops declare `double k`
+   and then an `int k` loop index over z, so the bulk modulus it assigns
+   (k = lambda + 2/3 G, lines 519-524) lands in the loop index: the modulus
+   passed to plastic_flow is truncated to an integer, and the z loop continues
+   from that integer + 1.  A column therefore visits its first node, then
+   trunc(K) + 1 and so on; the reference only finishes when every column
+   leaves the block this way (in 2D always, in 3D normally after the first z
+   node).  This follows that control flow node by node and reports the
+   columns where the reference would loop for ever. */
+static int calc_plastic(orc_problem *p, block_t *b, double dt) {
     const long n0 = p->nxd[0];
     double *F = p->f;
     const int pt = p->plastic_tensor;
     int st, o;
     if (p->ndim == 3) { st = 3; o = 9; } else if (p->mode == 2) { st = 2; o = 6; } else { st = 1; o = 3; }
-    double k = b->lam + 2. / 3. * b->g, g = b->g;
     for (int i = b->mlb[0]; i < b->prb[0]; i++)
-        for (int j = b->mlb[1]; j < b->prb[1]; j++)
+        for (int j = b->mlb[1]; j < b->prb[1]; j++) {
+            int visits = 0;
             for (int kk = b->mlb[2]; kk < b->prb[2]; kk++) {
+                if (++visits > p->nx[2] + 1) {
+                    snprintf(p->err, sizeof p->err,
+                             "the reference's plastic update does not terminate at column (%d, %d) of a block", i, j);
+                    return 0;
+                }
                 long id = (long)i * p->nxd[1] + (long)j * p->nxd[2] + kk;
+                double kb = b->lam + 2. / 3. * b->g, g = b->g;
+                if (p->hetmat) { /* block.cpp:519-521 */
+                    kb = p->mat[n0 + id] + 2. / 3. * p->mat[2 * n0 + id];
+                    g = p->mat[2 * n0 + id];
+                }
+                if (!(kb < 2147483647.)) {
+                    snprintf(p->err, sizeof p->err, "bulk modulus out of the range of the reference's int loop index");
+                    return 0;
+                }
+                const int kint = (int)kb;
+                const double k = (double)kint;
                 plastp in;
                 memset(&in, 0, sizeof in);
                 if (p->ndim == 3) {
@@ -1480,7 +1546,10 @@ static void calc_plastic(orc_problem *p, block_t *b, double dt) {
                     F[(o + 5) * n0 + id] = out.epyy; F[(o + 6) * n0 + id] = out.epyz; F[(o + 7) * n0 + id] = out.epzz;
                 }
                 (void)st;
+                kk = kint;
             }
+        }
+    return 1;
 }
 
 /* fields::set_stress / remove_stress: src/fields.cpp:184-220 */
@@ -1521,7 +1590,8 @@ int orc_do_rk_stage(orc_problem *p, double dt, int stage, double t) {
     for (long i = 0; i < ndf; i++) p->f[i] += B * p->df[i];
     if (stage + 1 == p->nstages && p->is_plastic) {
         orc_set_stress(p);
-        for (int b = 0; b < p->nbt; b++) calc_plastic(p, &p->blocks[b], dt);
+        for (int b = 0; b < p->nbt; b++)
+            if (!calc_plastic(p, &p->blocks[b], dt)) return 3;
         orc_remove_stress(p);
         for (int i = 0; i < p->nifaces; i++)
             if (!iface_apply(p, &p->ifaces[i], dt, tc, 1)) return 2;
@@ -1861,8 +1931,10 @@ static int load_all(orc_problem *p) {
     rd_str(&r, p->matfile, sizeof p->matfile);
     p->plastic_tensor = rd_int(&r);
     rd_close(&r);
-    if (strcmp(p->matfile, "none") != 0) {
-        snprintf(p->err, sizeof p->err, "heterogeneous material files are not supported by the oracle");
+    if (strcmp(p->matfile, "none") != 0 && p->ndim == 2 && p->mode == 3) {
+        /* the reference's time step reads a third material array that mode III
+           does not have (block.cpp:387-388, fields.cpp:58-61) */
+        snprintf(p->err, sizeof p->err, "heterogeneous material files are not supported for mode III");
         return 0;
     }
     int nfields, nfieldsp;
@@ -1905,6 +1977,19 @@ static int load_all(orc_problem *p) {
             snprintf(p->err, sizeof p->err, "Error opening stress file %s", p->loadfile);
             return 0;
         }
+    }
+    if (strcmp(p->matfile, "none") != 0) {
+        p->hetmat = 1;
+        p->mat = zalloc(3L * n);
+        if (!read_doubles(p->matfile, p->mat, 3L * n, 0)) {
+            snprintf(p->err, sizeof p->err, "Error opening material file %s", p->matfile);
+            return 0;
+        }
+        for (long q = 0; q < 3L * n; q++)
+            if (!(p->mat[q] > 0.)) { /* fields.cpp:648 */
+                snprintf(p->err, sizeof p->err, "material properties must be positive (%s)", p->matfile);
+                return 0;
+            }
     }
     /* operator: block.cpp:87-107 */
     p->cdiss = 0.;
@@ -1980,6 +2065,7 @@ static int load_all(orc_problem *p) {
             for (int j = b->mlb[1]; j < b->prb[1]; j++)
                 for (int k = b->mlb[2]; k < b->prb[2]; k++) {
                     long id = (long)i * p->nxd[1] + (long)j * p->nxd[2] + k;
+                    if (p->hetmat) cs = sqrt(p->mat[2 * n + id] / p->mat[id]);
                     for (int l = 0; l < p->ndim; l++) {
                         double dxt = 0.;
                         for (int m = 0; m < p->ndim; m++) {
@@ -2040,7 +2126,7 @@ orc_problem *orc_load(const char *infile, char *err, int errlen) {
 
 void orc_free(orc_problem *p) {
     if (!p) return;
-    free(p->f); free(p->df); free(p->x); free(p->metric); free(p->jac); free(p->s);
+    free(p->f); free(p->df); free(p->x); free(p->metric); free(p->jac); free(p->s); free(p->mat);
     for (int i = 0; i < 3; i++) {
         free(p->nx_block[i]);
         free(p->xm_block[i]);

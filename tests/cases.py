@@ -117,6 +117,36 @@ def c_m2_het(tmp):
     return p
 
 
+def c_m2_hetmat(tmp):
+    p = _m2("m2_hetmat")
+    P.layered_material(p, os.path.join(tmp, "m2_hetmat.mat"), seed=11)
+    return p
+
+
+def _yielding(p, mu, tensor):
+    """Plastic problem that yields: a uniform initial shear stress of 60 MPa
+    under 120 MPa compression puts the volume at the Drucker-Prager limit for
+    mu = 0.5 (no cohesion); the fault carries 10 MPa more shear."""
+    p = _plastic(p, tensor)
+    for b in p.blocks.values():
+        b.plastic = (mu, 0.0, 0.2, 0.01 * b.g)
+    p.s0 = (-120., 60., 0., -120., 0., -120.)
+    p.interfaces[0].loads[0] = P.load("constant", 0., 0., 0., 0., 0., 0., 10., 0.)
+    return p
+
+
+def c_m2_hetmat_plastic(tmp):
+    # yields at most nodes
+    p = _yielding(_m2("m2_hetmat_plastic"), 0.5, False)
+    P.layered_material(p, os.path.join(tmp, "m2_hetmat_plastic.mat"), seed=12)
+    return p
+
+
+def c_m2_plastic_yield(tmp):
+    # yields at a few nodes near the rupture front
+    return _yielding(_m2("m2_plastic_yield"), 0.51, True)
+
+
 def c_m2_plastic(tmp):
     p = _plastic(_m2("m2_plastic"))
     p.s0 = (-120., 0., 0., -120., 0., -120.)
@@ -208,6 +238,17 @@ def c_p3_plastic(tmp):
     return p
 
 
+def c_p3_hetmat(tmp):
+    p = _p3("p3_hetmat", tmp)
+    p.blocks[(0, 0, 0)].bounds = ["absorbing", "free", "absorbing", "none", "free", "absorbing"]
+    P.layered_material(p, os.path.join(tmp, "p3_hetmat.mat"), seed=13)
+    return p
+
+
+def c_p3_plastic_yield(tmp):
+    return _yielding(_p3("p3_plastic_yield", tmp, nt=10), 0.5, True)
+
+
 def c_p3_stz(tmp):
     p = _p3("p3_stz", tmp, nt=12)
     itf = p.interfaces[0]
@@ -287,7 +328,8 @@ CASES: Dict[str, Callable] = {
     "m3": c_m3, "m3_plastic": c_m3_plastic, "m2_stz": c_m2_stz, "m2_four_blocks": c_m2_four_blocks,
     "p3_sw": c_p3_sw, "p3_rk4": c_p3_rk4, "p3_plastic": c_p3_plastic, "p3_stz": c_p3_stz,
     "p3_xfault": c_p3_xfault, "p3_zfault": c_p3_zfault, "p3_stz_files": c_p3_stz_files,
-    "p3_rough": c_p3_rough,
+    "p3_rough": c_p3_rough, "m2_hetmat": c_m2_hetmat, "m2_hetmat_plastic": c_m2_hetmat_plastic,
+    "p3_hetmat": c_p3_hetmat, "m2_plastic_yield": c_m2_plastic_yield, "p3_plastic_yield": c_p3_plastic_yield,
 }
 
 # cases whose friction law calls exp/log inside the per-stage solve (STZ);

@@ -45,6 +45,8 @@ def test_create_rejects_missing_file(tmp_path):
     (lambda p: setattr(p, "sbporder", 5), b"sbporder"),
     (lambda p: setattr(p.interfaces[0], "kind", "bogus"), b"interface type"),
     (lambda p: setattr(p, "nx_block", ([61], [31, 10], [1])), b"too few points"),
+    # the reference's time step would read a third material array mode III lacks
+    (lambda p: (setattr(p, "mode", 3), setattr(p, "matfile", "m.mat")), b"mode III"),
 ])
 def test_create_rejects_invalid_problem(tmp_path, mutate, message):
     p = P.mode2_rupture(nx=61, ny=31, nt=5, datadir=str(tmp_path) + "/")

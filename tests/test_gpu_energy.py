@@ -10,7 +10,7 @@
 * Energy stability of the semi-discretisation: from random states without
   initial stress or loads, dE/dt <= 0 for absorbing, free and rigid outer
   faces, locked, frictionless and slip-weakening interfaces, SBP orders 2-4,
-  2D (modes II and III) and 3D.
+  2D (modes II and III) and 3D, homogeneous and heterogeneous material.
 * Over one RK step of a running rupture the energy change matches the
   trapezoidal rule on the computed rates.
 * The FP32 path's energies against the FP64 path's after a rupture.
@@ -91,6 +91,8 @@ def node_weights(prob):
 
 def energy_numpy(prob, J, F, R):
     rho, lam, g = P.RHO, P.LAM, P.G
+    if prob.matfile != "none":   # per-node material
+        rho, lam, g = np.fromfile(prob.matfile, dtype="<f8").reshape(3, -1)
     w = node_weights(prob) * J
     z = np.zeros_like(F[0])
     if prob.ndim == 3:
@@ -119,7 +121,7 @@ def write(prob, tmp):
     return prob.write(os.path.join(tmp, prob.name + ".in"))
 
 
-@pytest.mark.parametrize("name", ["m2_sw", "m3", "p3_sw", "m2_s2rk4", "m2_s3rk2"])
+@pytest.mark.parametrize("name", ["m2_sw", "m3", "p3_sw", "m2_s2rk4", "m2_s3rk2", "m2_hetmat", "p3_hetmat"])
 def test_energy_reductions_match_numpy(tmp_path, name):
     prob = build_case(name, str(tmp_path), outputs=False)
     with fs.Problem(write(prob, str(tmp_path)), precision=fs.FP64) as p:
@@ -148,7 +150,7 @@ def _unloaded(name, tmp):
 
 
 @pytest.mark.parametrize("name", ["m2_sw", "m2_freerigid", "m2_locked", "m2_frictionless", "m3", "p3_sw",
-                                  "p3_rk4", "m2_s2rk4", "m2_s3rk2"])
+                                  "p3_rk4", "m2_s2rk4", "m2_s3rk2", "m2_hetmat", "p3_hetmat"])
 def test_energy_rate_nonpositive_without_sources(tmp_path, name):
     prob = _unloaded(name, str(tmp_path))
     rng = np.random.default_rng(17)

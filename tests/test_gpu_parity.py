@@ -64,7 +64,8 @@ def test_fp64_matches_reference(name, tmp_path):
             assert np.array_equal(a, b), "%s max diff %g" % (key, np.max(np.abs(a - b)))
 
 
-@pytest.mark.parametrize("name", ["m2_sw", "p3_sw", "m2_plastic", "p3_plastic", "m3", "m2_four_blocks"])
+@pytest.mark.parametrize("name", ["m2_sw", "p3_sw", "m2_plastic", "p3_plastic", "m3", "m2_four_blocks", "m2_hetmat",
+                                  "p3_hetmat", "m2_hetmat_plastic", "m2_plastic_yield", "p3_plastic_yield"])
 def test_fp64_stage_from_random_state(name, tmp_path):
     """One stage (A != 0) from a random state: fields, rates and fault arrays identical."""
     prob = cases.build_case(name, str(tmp_path), outputs=False)
@@ -105,7 +106,8 @@ def test_fp64_stage_from_random_state(name, tmp_path):
 
 
 @pytest.mark.parametrize("name", ["m2_sw", "m2_freerigid", "m2_plastic", "m3", "p3_sw", "p3_rk4", "p3_plastic",
-                                  "p3_xfault", "p3_zfault"])
+                                  "p3_xfault", "p3_zfault", "m2_hetmat", "p3_hetmat", "m2_plastic_yield",
+                                  "p3_plastic_yield"])
 def test_fp32_close_to_reference(name, tmp_path):
     prob, got = run_solve(name, str(tmp_path), fs.FP32)
     gold = helpers.load_golden(name)
