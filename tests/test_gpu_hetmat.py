@@ -35,7 +35,9 @@ def fields(p):
     return np.array([p.field(c) for c in range(p.nfields + p.nfieldsp)])
 
 
-@pytest.mark.parametrize("name", ["m2_sw", "p3_sw", "m2_plastic_yield"])
+# (not mode II plastic: with a material file the reference's sigma_zz rate
+# takes its second modulus from the next x row's density, block.cpp:1289-1291)
+@pytest.mark.parametrize("name", ["m2_sw", "p3_sw", "p3_plastic_yield"])
 def test_uniform_material_file_matches_homogeneous(tmp_path, name):
     tmp = str(tmp_path)
     prob = cases.build_case(name, tmp, outputs=False)
