@@ -17,8 +17,9 @@
 //    planes near the block's x faces, whose closure rows reach 3H planes,
 //    read their taps straight from global memory;
 //  * the y and z derivative inputs of the centre plane go to shared tiles
-//    with an (order-1) halo; halo nodes are loaded a plane ahead into
-//    registers by the threads that own them;
+//    with an (order-1) halo.  The centre boxes are staged 4 columns wider on
+//    each side, so the k halo comes from the stage; the j halo rows are loaded
+//    a plane ahead into registers by the threads that own them;
 //  * interior stencils are unrolled in the antisymmetric form with immediate
 //    coefficients; y closure rows (whole warps) use the tabulated rows and
 //    the two k-edge tiles use one tap row per lane, as in stage_fast.cu;
@@ -28,8 +29,9 @@
 //    the plane and finish k-face nodes themselves, so their stores stay whole
 //    rows; nodes on x or y faces are written without those faces' SATs and
 //    finished by the face-node kernel of stage_fast.cu (coalesced along k).
-// Each staged box is one tensor copy over a (k, j, i, component) map whose k
-// origin is the 16-byte boundary at or below the tile's first column.  Every
+// Each staged box is one tensor copy over a (k, j, i, component) map.  Tiles
+// start on 4-column (16-byte) boundaries: the last tile of a row is moved up
+// to one and its columns past the block face are computed and dropped.  Every
 // mbarrier wait is bounded: on expiry the CTA records FDF_ERR_TIMEOUT, waits
 // (bounded) for the copies it still has in flight and returns.
 #include <cuda.h>
@@ -51,7 +53,8 @@ namespace fdf {
 // tensor maps of the FP32 arrays for kind 3 (F: both field buffers; M9: the
 // nine metric rows; M3: the x metric rows; DF: the rate register)
 struct RegMaps {
-    CUtensorMap F[2], M9, M3, J, DF;
+    CUtensorMap F[2], M9, J;        // centre plane: 4 halo columns on each side
+    CUtensorMap FL[2], M3, JL, DF;  // leading plane and rate register: the tile's columns
 };
 
 struct RegMapsHost {
@@ -70,7 +73,9 @@ struct RegMapsHost {
 namespace {
 
 constexpr int TJ = 8, TK = 32, NT = TJ * TK;
-constexpr int SW = TK + 4;   // staged row: 16-byte boundary at or below the tile's first column, 36 floats
+constexpr int KH = 4;             // halo columns staged on each side of the centre boxes (>= H, 16 bytes)
+constexpr int SWC = TK + 2 * KH;  // staged centre row, 40 floats
+constexpr int SWD = TK;           // staged row of the rate register and the leading plane
 
 constexpr int up32(int n) { return (n + 31) / 32 * 32; }   // every box on a 128-byte boundary
 constexpr int KBJ = TJ + 4;   // staged k-face row: 16-byte boundary at or below the tile's first j
@@ -79,14 +84,14 @@ template <int ORDER>
 struct RgCfg {
     static constexpr int H = ORDER - 1, NB = 2 * H, NTB = 3 * H, W = 2 * H + 1;
     static constexpr int VH = TJ + 2 * H, VW = TK + 2 * H;
-    static constexpr int BOX = TJ * SW;   // floats of one staged component
-    // stage layout, floats: centre F[9], M[9], J, DF[9]; leading F[9], Mx[3], J
-    // k-edge tiles also stage their rows of the k-face SAT increments: per
-    // face side one box of KBJ j x 9 components
-    static constexpr int CF = 0, CM = CF + up32(9 * BOX), CJ = CM + up32(9 * BOX), CD = CJ + up32(BOX),
-                         LF = CD + up32(9 * BOX), LM = LF + up32(9 * BOX), LJ = LM + up32(3 * BOX),
-                         KSW = up32(9 * KBJ), KS = LJ + up32(BOX), SSZ = KS + 2 * KSW;
-    static constexpr uint32_t BYTES = 4u * 41 * BOX, KBYTES = 4u * 9 * KBJ;
+    static constexpr int BOXC = TJ * SWC, BOXD = TJ * SWD;   // floats of one staged component
+    // stage layout, floats: centre F[9], M[9], J (BOXC each); DF[9], leading
+    // F[9], Mx[3], J (BOXD each).  k-edge tiles also stage their rows of the
+    // k-face SAT increments: per face side one box of KBJ j x 9 components
+    static constexpr int CF = 0, CM = CF + up32(9 * BOXC), CJ = CM + up32(9 * BOXC), CD = CJ + up32(BOXC),
+                         LF = CD + up32(9 * BOXD), LM = LF + up32(9 * BOXD), LJ = LM + up32(3 * BOXD),
+                         KSW = up32(9 * KBJ), KS = LJ + up32(BOXD), SSZ = KS + 2 * KSW;
+    static constexpr uint32_t BYTES = 4u * (19 * BOXC + 22 * BOXD), KBYTES = 4u * 9 * KBJ;
     static constexpr int TY = 3 * VH * TK, TZ = 3 * TJ * VW;   // float2
     static constexpr int WROWS = 2 * NB + 1;
     static constexpr int WTAB = ((WROWS * NTB + 3) / 4) * 4;
@@ -120,7 +125,8 @@ __global__ void __launch_bounds__(NT, 2)
     k_reg3d(VolumeArgs<float> a, BlockDev B, StageArgs sa, int chunk, int* status,
             const __grid_constant__ RegMaps maps, int fsel, const __grid_constant__ CUtensorMap kmap) {
     using C = RgCfg<ORDER>;
-    constexpr int H = C::H, NB = C::NB, NTB = C::NTB, W = C::W, VH = C::VH, VW = C::VW, BOX = C::BOX;
+    constexpr int H = C::H, NB = C::NB, NTB = C::NTB, W = C::W, VH = C::VH, VW = C::VW, BOXC = C::BOXC,
+                  BOXD = C::BOXD;
     extern __shared__ __align__(128) float smem[];
     float* stg = smem;                                            // two stages of C::SSZ floats
     float2* ty = reinterpret_cast<float2*>(smem + 2 * C::SSZ);   // [3][VH][TK]  (F_y,c , v_c)
@@ -133,13 +139,14 @@ __global__ void __launch_bounds__(NT, 2)
     const int n0 = B.n[0], n1 = B.n[1], n2 = B.n[2];
     const int tid = threadIdx.x;
     const int tk = tid % TK, tj = tid / TK;
-    // tiles and ownership as in stage_fast.cu: the last tile in j and k ends
-    // on the block face and owns the closure rows near it
+    // tiles and ownership as in stage_fast.cu: the last tile in j ends on the
+    // block face, the last tile in k at or up to 3 columns past it (its first
+    // column on a 4-column boundary); each owns the closure rows near its face
     const bool lastk = blockIdx.x == gridDim.x - 1, lastj = blockIdx.y == gridDim.y - 1;
-    const int k0 = lastk ? n2 - TK : blockIdx.x * TK;
+    const int k0 = lastk ? ((n2 - TK + 3) & ~3) : blockIdx.x * TK;
     const int j0 = lastj ? n1 - TJ : blockIdx.y * TJ;
     const int k = k0 + tk, j = j0 + tj;
-    const bool ownk = (k >= n2 - NB) ? lastk : (k / TK == (int)blockIdx.x);
+    const bool ownk = (k >= n2) ? false : (k >= n2 - NB) ? lastk : (k / TK == (int)blockIdx.x);
     const bool ownj = (j >= n1 - NB) ? lastj : (j / TJ == (int)blockIdx.y);
     const bool owner = ownk && ownj;
     const int ib = blockIdx.z * chunk;
@@ -147,12 +154,12 @@ __global__ void __launch_bounds__(NT, 2)
     if (ib >= ie) return;
     const long long wlim = sa.wait_limit > 0 ? sa.wait_limit : (1LL << 22);
 
-    // staged boxes: k origin at the 16-byte boundary at or below the tile
+    // staged boxes: the tile's first column kg is on a 16-byte boundary (the
+    // block's first k is, by the support check); centre boxes start KH before it
     const int kg = B.lo[2] + k0;
-    const int kofs = kg & 3;
-    const int kgb = kg - kofs;
     const int jg = B.lo[1] + j0;
     const CUtensorMap* mF = &maps.F[fsel];
+    const CUtensorMap* mFL = &maps.FL[fsel];
     const uint32_t bar0 = saddr(bars), bar1 = saddr(bars + 1);
     // warp-arrival barriers of the march (one arrival per warp and plane):
     // flux tiles written, flux tiles read, stage consumed
@@ -195,13 +202,13 @@ __global__ void __launch_bounds__(NT, 2)
         const int ig = B.lo[0] + i;
         fence_proxy_async();
         bar_expect(bar, bytes);
-        tma4(saddr(st + C::CF), mF, kgb, jg, ig, 0, bar);
-        tma4(saddr(st + C::CM), &maps.M9, kgb, jg, ig, 0, bar);
-        tma3(saddr(st + C::CJ), &maps.J, kgb, jg, ig, bar);
-        tma4(saddr(st + C::CD), &maps.DF, kgb, jg, ig, 0, bar);
-        tma4(saddr(st + C::LF), mF, kgb, jg, ig + H, 0, bar);
-        tma4(saddr(st + C::LM), &maps.M3, kgb, jg, ig + H, 0, bar);
-        tma3(saddr(st + C::LJ), &maps.J, kgb, jg, ig + H, bar);
+        tma4(saddr(st + C::CF), mF, kg - KH, jg, ig, 0, bar);
+        tma4(saddr(st + C::CM), &maps.M9, kg - KH, jg, ig, 0, bar);
+        tma3(saddr(st + C::CJ), &maps.J, kg - KH, jg, ig, bar);
+        tma4(saddr(st + C::CD), &maps.DF, kg, jg, ig, 0, bar);
+        tma4(saddr(st + C::LF), mFL, kg, jg, ig + H, 0, bar);
+        tma4(saddr(st + C::LM), &maps.M3, kg, jg, ig + H, 0, bar);
+        tma3(saddr(st + C::LJ), &maps.JL, kg, jg, ig + H, bar);
         if (kf0) tma3(saddr(st + C::KS), &kmap, kjb, i, 0, bar);
         if (kf1) tma3(saddr(st + C::KS + C::KSW), &kmap, kjb, i, 9, bar);
     };
@@ -251,16 +258,16 @@ __global__ void __launch_bounds__(NT, 2)
         if (gj < 0 || gj >= n1 || gk < 0 || gk >= n2) hkind = -1;
     }
     const int hbase = B.lo[0] * s0 + (B.lo[1] + j0 + hj) * (int)L.s1 + (B.lo[2] + k0 + hk);
-    const int hrow = (hkind == 0) ? 3 : 6;   // metric row y or z
+    // j-halo nodes: loaded a plane ahead from global memory (metric rows 3-5)
     auto load_halo = [&](int i, HaloNode& h) {
-        if (hkind < 0) return;
+        if (hkind != 0) return;
         const int id = hbase + i * s0;
 #pragma unroll
         for (int c = 0; c < 6; c++) h.s[c] = __ldg(F + (3 + c) * cs + id);
 #pragma unroll
         for (int c = 0; c < 3; c++) h.v[c] = __ldg(F + c * cs + id);
 #pragma unroll
-        for (int c = 0; c < 3; c++) h.m[c] = __ldg(M + (hrow + c) * cs + id);
+        for (int c = 0; c < 3; c++) h.m[c] = __ldg(M + (3 + c) * cs + id);
         h.J = __ldg(Jg + id);
     };
     // x flux and velocity of this thread's column at plane q, from global memory
@@ -312,7 +319,9 @@ __global__ void __launch_bounds__(NT, 2)
     HaloNode hn;
     load_halo(ib, hn);
 
-    const int so = tj * SW + tk + kofs;   // this node in a staged component
+    const int so = tj * SWC + tk + KH;   // this node in a staged centre component
+    const int sod = tj * SWD + tk;       // ... in a staged rate or leading-plane component
+    const int hso = hj * SWC + hk + KH;  // the k-halo node in a staged centre component
     for (int i = ib; i < ie; i++) {
         const int kk = i - ib;
         const int b = kk & 1;
@@ -334,27 +343,31 @@ __global__ void __launch_bounds__(NT, 2)
         {
             float s[6], Fy[3], Fz[3];
 #pragma unroll
-            for (int c = 0; c < 6; c++) s[c] = st[C::CF + (3 + c) * BOX + so];
+            for (int c = 0; c < 6; c++) s[c] = st[C::CF + (3 + c) * BOXC + so];
             const float Jc = st[C::CJ + so];
-            fluxes(Jc, st[C::CM + 3 * BOX + so], st[C::CM + 4 * BOX + so], st[C::CM + 5 * BOX + so], s, Fy);
-            fluxes(Jc, st[C::CM + 6 * BOX + so], st[C::CM + 7 * BOX + so], st[C::CM + 8 * BOX + so], s, Fz);
+            fluxes(Jc, st[C::CM + 3 * BOXC + so], st[C::CM + 4 * BOXC + so], st[C::CM + 5 * BOXC + so], s, Fy);
+            fluxes(Jc, st[C::CM + 6 * BOXC + so], st[C::CM + 7 * BOXC + so], st[C::CM + 8 * BOXC + so], s, Fz);
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                const float v = st[C::CF + c * BOX + so];
+                const float v = st[C::CF + c * BOXC + so];
                 ty[(c * VH + tj + H) * TK + tk] = make_float2(Fy[c], v);
                 tz[(c * TJ + tj) * VW + tk + H] = make_float2(Fz[c], v);
             }
         }
-        if (hkind >= 0) {
+        if (hkind == 0) {
             float Fh[3];
             fluxes(hn.J, hn.m[0], hn.m[1], hn.m[2], hn.s, Fh);
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                if (hkind == 0)
-                    ty[(c * VH + hj + H) * TK + hk] = make_float2(Fh[c], hn.v[c]);
-                else
-                    tz[(c * TJ + hj) * VW + hk + H] = make_float2(Fh[c], hn.v[c]);
-            }
+            for (int c = 0; c < 3; c++) ty[(c * VH + hj + H) * TK + hk] = make_float2(Fh[c], hn.v[c]);
+        } else if (hkind == 1) {   // k halo: from the staged centre boxes
+            float s[6], Fh[3];
+#pragma unroll
+            for (int c = 0; c < 6; c++) s[c] = st[C::CF + (3 + c) * BOXC + hso];
+            fluxes(st[C::CJ + hso], st[C::CM + 6 * BOXC + hso], st[C::CM + 7 * BOXC + hso],
+                   st[C::CM + 8 * BOXC + hso], s, Fh);
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+                tz[(c * TJ + hj) * VW + hk + H] = make_float2(Fh[c], st[C::CF + c * BOXC + hso]);
         }
         __syncwarp();
         if (lane == 0) bar_arrive(barT);
@@ -365,10 +378,10 @@ __global__ void __launch_bounds__(NT, 2)
         if (i + H < n0) {
             float s[6], v[3], Fx[3];
 #pragma unroll
-            for (int c = 0; c < 6; c++) s[c] = st[C::LF + (3 + c) * BOX + so];
+            for (int c = 0; c < 6; c++) s[c] = st[C::LF + (3 + c) * BOXD + sod];
 #pragma unroll
-            for (int c = 0; c < 3; c++) v[c] = st[C::LF + c * BOX + so];
-            fluxes(st[C::LJ + so], st[C::LM + so], st[C::LM + BOX + so], st[C::LM + 2 * BOX + so], s, Fx);
+            for (int c = 0; c < 3; c++) v[c] = st[C::LF + c * BOXD + sod];
+            fluxes(st[C::LJ + sod], st[C::LM + sod], st[C::LM + BOXD + sod], st[C::LM + 2 * BOXD + sod], s, Fx);
 #pragma unroll
             for (int m = 0; m < W - 1; m++)
 #pragma unroll
@@ -475,7 +488,7 @@ __global__ void __launch_bounds__(NT, 2)
         // ---- rate: df = A df + L(f), then the RK update
         float df[9];
 #pragma unroll
-        for (int c = 0; c < 9; c++) df[c] = st[C::CD + c * BOX + so];
+        for (int c = 0; c < 9; c++) df[c] = st[C::CD + c * BOXD + sod];
         const float iJ = __frcp_rn(st[C::CJ + so]);
         {
             const float w0 = crho[0] * iJ, w1 = crho[1] * iJ, w2 = crho[2] * iJ;
@@ -491,7 +504,7 @@ __global__ void __launch_bounds__(NT, 2)
                 for (int c = 0; c < 3; c++) Dv[d][c] *= sd[d];
             float m[9];
 #pragma unroll
-            for (int c = 0; c < 9; c++) m[c] = st[C::CM + c * BOX + so];
+            for (int c = 0; c < 9; c++) m[c] = st[C::CM + c * BOXC + so];
             float e[3][3];
 #pragma unroll
             for (int va = 0; va < 3; va++)
@@ -518,7 +531,7 @@ __global__ void __launch_bounds__(NT, 2)
             // x/y face nodes: k_faces3d adds those SATs and finishes them
             if (!(facexy | (i == 0) | (i == n0 - 1) | (kface == 2))) {
 #pragma unroll
-                for (int c = 0; c < 9; c++) Fn[c * cs + id] = fmaf(Bcoef, df[c], st[C::CF + c * BOX + so]);
+                for (int c = 0; c < 9; c++) Fn[c * cs + id] = fmaf(Bcoef, df[c], st[C::CF + c * BOXC + so]);
             }
         }
         __syncwarp();
@@ -607,14 +620,18 @@ RegMapsHost* make_reg_maps(const Layout& L, const float* F0, const float* F1, co
     const cuuint64_t d4[4] = {(cuuint64_t)L.s1, (cuuint64_t)L.nx[1], (cuuint64_t)L.nx[0], 9};
     const cuuint64_t s4[3] = {(cuuint64_t)L.s1 * 4, (cuuint64_t)L.s0 * 4, (cuuint64_t)L.cstride * 4};
     const cuuint64_t d3[3] = {(cuuint64_t)L.s1, (cuuint64_t)L.nx[1], (cuuint64_t)L.nx[0]};
-    const cuuint32_t b9[4] = {SW, TJ, 1, 9}, b3[4] = {SW, TJ, 1, 3}, b1[3] = {SW, TJ, 1};
+    const cuuint32_t c9[4] = {SWC, TJ, 1, 9}, c1[3] = {SWC, TJ, 1};
+    const cuuint32_t d9[4] = {SWD, TJ, 1, 9}, d3b[4] = {SWD, TJ, 1, 3}, d1[3] = {SWD, TJ, 1};
     try {
-        tma_encode(&h->m.F[0], F0, 4, d4, s4, b9);
-        tma_encode(&h->m.F[1], F1, 4, d4, s4, b9);
-        tma_encode(&h->m.M9, M, 4, d4, s4, b9);
-        tma_encode(&h->m.M3, M, 4, d4, s4, b3);
-        tma_encode(&h->m.J, J, 3, d3, s4, b1);
-        tma_encode(&h->m.DF, DF, 4, d4, s4, b9);
+        tma_encode(&h->m.F[0], F0, 4, d4, s4, c9);
+        tma_encode(&h->m.F[1], F1, 4, d4, s4, c9);
+        tma_encode(&h->m.M9, M, 4, d4, s4, c9);
+        tma_encode(&h->m.J, J, 3, d3, s4, c1);
+        tma_encode(&h->m.FL[0], F0, 4, d4, s4, d9);
+        tma_encode(&h->m.FL[1], F1, 4, d4, s4, d9);
+        tma_encode(&h->m.M3, M, 4, d4, s4, d3b);
+        tma_encode(&h->m.JL, J, 3, d3, s4, d1);
+        tma_encode(&h->m.DF, DF, 4, d4, s4, d9);
         h->ksat.assign(nblocks, nullptr);
         h->jp.assign(nblocks, 0);
         h->kmap.resize(nblocks);
@@ -649,6 +666,7 @@ bool reg3d_supported(const Layout& L, const BlockDev& b, int order) {
     if (b.n[0] < 4 * order - 3) return false;
     if (L.cstride * 9 >= (1LL << 31)) return false;   // 32-bit element offsets
     if (L.s1 % 4 != 0 || L.s0 % 4 != 0 || L.cstride % 4 != 0) return false;   // 16-byte row starts
+    if (b.lo[2] % 4 != 0) return false;   // tiles start on 16-byte boundaries
     return true;
 }
 
