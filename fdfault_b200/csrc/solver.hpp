@@ -96,7 +96,7 @@ class Solver {
     int volume_kernel_active() const;   // the kind that runs (0 when the chosen one does not apply)
     // polls of a bounded wait for staged data (<= 0: the built-in limit)
     void set_wait_limit(long long polls) {
-        wait_limit_ = polls > 0 ? polls : (1LL << 22);
+        wait_limit_ = polls != 0 ? polls : (1LL << 22);
         graph_dirty_ = true;
     }
     // replay steps from a captured CUDA graph of two steps (default on)

@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(NT, 2)
     const int ib = blockIdx.z * chunk;
     const int ie = min(n0, ib + chunk);
     if (ib >= ie) return;
-    const long long wlim = sa.wait_limit > 0 ? sa.wait_limit : (1LL << 22);
+    const long long wlim = sa.wait_limit != 0 ? sa.wait_limit : (1LL << 22);
 
     // staged boxes: the tile's first column kg is on a 16-byte boundary (the
     // block's first k is, by the support check); centre boxes start KH before it

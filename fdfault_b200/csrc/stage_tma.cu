@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(NT, 1)
     const int ib = blockIdx.z * chunk;
     const int ie = min(n0, ib + chunk);
     if (ib >= ie) return;
-    const long long wlim = sa.wait_limit > 0 ? sa.wait_limit : (1LL << 22);
+    const long long wlim = sa.wait_limit != 0 ? sa.wait_limit : (1LL << 22);
 
     const int s0 = (int)L.s0, s1 = (int)L.s1;
     const int colbase = B.lo[0] * s0 + (B.lo[1] + j) * s1 + (B.lo[2] + k);

@@ -54,8 +54,10 @@ __device__ __forceinline__ bool bar_test(uint32_t bar, uint32_t parity) {
 constexpr long long TMA_DRAIN_LIMIT = 1LL << 24;
 // wait for phase `parity` of the barrier; false when `limit` polls pass first.
 // The first poll never blocks, the later ones may suspend the thread for a
-// while (mbarrier.try_wait), so a limit of 1 is one immediate test.
+// while (mbarrier.try_wait), so a limit of 1 is one immediate test; a
+// negative limit gives up at once without looking (the expiry path on demand).
 __device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity, long long limit) {
+    if (limit < 0) return false;
     if (bar_test(bar, parity)) return true;
     for (long long it = 1; it < limit; it++)
         if (bar_try(bar, parity)) return true;

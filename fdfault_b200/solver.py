@@ -312,7 +312,8 @@ class Problem:
 
     def set_wait_limit(self, polls: int) -> None:
         """Polls of each bounded wait for staged data in volume kernels 2 and 3
-        (<= 0: the built-in limit); 1 makes every wait a single immediate test."""
+        (0: the built-in limit); 1 makes every wait a single immediate test,
+        a negative value makes every such wait give up at once."""
         self._check(self._L.fdf_set_wait_limit(self._h, polls))
 
     def use_fast_kernel(self, on: bool) -> bool:

@@ -156,13 +156,14 @@ int fdf_use_fast_kernel(fdf_handle* h, int on, int* active);
 int fdf_set_volume_kernel(fdf_handle* h, int kind, int* active);
 
 /* Polls of each bounded wait for staged data in the TMA-staged volume kernels
- * (kinds 2 and 3); polls <= 0 restores the built-in limit (2^22).  A wait that
+ * (kinds 2 and 3); polls = 0 restores the built-in limit (2^22).  A wait that
  * runs out makes its CTA record FDF_ERR_TIMEOUT in the device status word
  * (reported by the next fdf_synchronize as FDF_ERR_SOLVER), wait with a fixed
  * generous limit for its own copies still in flight, and return; the fields of
  * that stage are then incomplete.  With polls = 1 every wait is a single
- * immediate test, which lets a test exercise this path.  No reference
- * counterpart: the reference has no device waits. */
+ * immediate test; with polls < 0 every such wait gives up at once, so a test
+ * can exercise this path deterministically.  No reference counterpart: the
+ * reference has no device waits. */
 int fdf_set_wait_limit(fdf_handle* h, long long polls);
 
 /* Nodes and bulk modulus of the Drucker-Prager return map (plastic problems).

@@ -3,7 +3,7 @@ waits of the TMA-staged kernels, reach the host as a solver status from
 fdf_synchronize (FDF_ERR_SOLVER, with the status bits in the message), and the
 GPU stays usable afterwards.  Failures are made on the host side of the inputs
 (a NaN in a side file, an STZ melting threshold below the slip rate, a wait
-limit of one immediate test); nothing here faults or hangs a GPU.
+limit that gives up at once); nothing here faults or hangs a GPU.
 
 Reference abort sites: src/utilities.cpp:134-137,173-176 (Newton), src/stz.cpp:
 341-344 (slip rate above v1)."""
@@ -89,14 +89,14 @@ def _planar(tmp):
 
 @pytest.mark.parametrize("kind", [2, 3])
 def test_staged_wait_limit_reports_timeout(tmp_path, kind):
-    """With every wait reduced to one immediate test, CTAs whose data has not
-    landed give up: the status says so, each such CTA first waits for its own
-    copies, and a fresh handle on the same GPU then gives the normal results."""
+    """With every bounded wait giving up at once, the CTAs give up: the status
+    says so, each CTA first waits for its own copies in flight, and a fresh
+    handle on the same GPU then gives the normal results."""
     infile = _planar(str(tmp_path))
     with fs.Problem(infile, precision=fs.FP32) as p:
         assert p.set_volume_kernel(kind) == kind
         p.use_graphs(False)
-        p.set_wait_limit(1)
+        p.set_wait_limit(-1)
         p.step(1)
         with pytest.raises(fs.FdfaultError) as ei:
             p.synchronize()
