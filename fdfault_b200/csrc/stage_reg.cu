@@ -13,9 +13,7 @@
 //    the x fluxes J (m_x . sigma_c) and velocities enter the x window;
 //  * the x window of the interior stencil (planes i-H .. i+H of the thread's
 //    own column: three fluxes and three velocities each) lives in registers,
-//    so shared memory holds only the two stages and the y/z flux tiles; the
-//    planes near the block's x faces, whose closure rows reach 3H planes,
-//    read their taps straight from global memory;
+//    so shared memory holds only the two stages and the y/z flux tiles;
 //  * the y and z derivative inputs of the centre plane go to shared tiles
 //    with an (order-1) halo.  The centre boxes are staged 4 columns wider on
 //    each side, so the k halo comes from the stage; the j halo rows are loaded
@@ -23,6 +21,9 @@
 //  * interior stencils are unrolled in the antisymmetric form with immediate
 //    coefficients; y closure rows (whole warps) use the tabulated rows and
 //    the two k-edge tiles use one tap row per lane, as in stage_fast.cu;
+//  * the 2(order-1) planes at each x face, whose closure rows reach 3(order-1)
+//    planes, take their x derivatives from a pre-pass (k_xcl3d) that forms
+//    them from the stage-start fields in global memory;
 //  * outer SATs: a pre-pass (k_ksat3d, one thread per k-face node) evaluates
 //    the SAT increments of the two k faces from the stage-start fields into a
 //    compact per-block buffer; the k-edge tiles stage their rows of it with
@@ -64,8 +65,12 @@ struct RegMapsHost {
     std::vector<float*> ksat;
     std::vector<int> jp;
     std::vector<CUtensorMap> kmap;
+    // per block: x derivatives of the closure planes [slot][q][j][k] (see k_xcl3d)
+    std::vector<float*> xcl;
     ~RegMapsHost() {
         for (float* p : ksat)
+            if (p) cudaFree(p);
+        for (float* p : xcl)
             if (p) cudaFree(p);
     }
 };
@@ -123,7 +128,8 @@ __device__ __forceinline__ float2 fma2(float a, float2 x, float2 acc) { return _
 template <int ORDER>
 __global__ void __launch_bounds__(NT, 2)
     k_reg3d(VolumeArgs<float> a, BlockDev B, StageArgs sa, int chunk, int* status,
-            const __grid_constant__ RegMaps maps, int fsel, const __grid_constant__ CUtensorMap kmap) {
+            const __grid_constant__ RegMaps maps, int fsel, const __grid_constant__ CUtensorMap kmap,
+            const float* __restrict__ xcl) {
     using C = RgCfg<ORDER>;
     constexpr int H = C::H, NB = C::NB, NTB = C::NTB, W = C::W, VH = C::VH, VW = C::VW, BOXC = C::BOXC,
                   BOXD = C::BOXD;
@@ -400,20 +406,12 @@ __global__ void __launch_bounds__(NT, 2)
                 for (int n = 1; n <= H; n++) acc = fma2(inner_c<ORDER>(n), sub2(w[H + n][c], w[H - n][c]), acc);
                 D[0][c] = acc;
             }
-        } else {   // x closure rows: 3H taps from global memory
-            const bool left = i < NB;
-            const int row = left ? i + 1 : n0 - i;
-            const float sg = left ? 1.f : -1.f;
-            float2 acc[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-            for (int n = 0; n < NTB; n++) {
-                const float cf = sbp_coef<float>(ORDER, row, n);
-                float Fx[3], v[3];
-                direct(left ? n : n0 - 1 - n, Fx, v);
+        } else {   // x closure rows: from the pre-pass
+            const int slot = (i < NB) ? i : NB + i - (n0 - NB);
+            const long long pl = (long long)n1 * n2;
+            const float* xc = xcl + (long long)slot * 6 * pl + (long long)j * n2 + min(k, n2 - 1);
 #pragma unroll
-                for (int c = 0; c < 3; c++) acc[c] = fma2(cf, make_float2(Fx[c], v[c]), acc[c]);
-            }
-#pragma unroll
-            for (int c = 0; c < 3; c++) D[0][c] = __fmul2_rn(make_float2(sg, sg), acc[c]);
+            for (int c = 0; c < 3; c++) D[0][c] = make_float2(xc[2 * c * pl], xc[(2 * c + 1) * pl]);
         }
         // flux tiles of plane i complete; a wait that ran out anywhere ends the CTA
         if (!bar_wait(barT, kk & 1, TMA_DRAIN_LIMIT) || *abort_flag) {
@@ -563,6 +561,57 @@ __global__ void __launch_bounds__(128) k_ksat3d(VolumeArgs<float> a, BlockDev B,
     for (int c = 0; c < 9; c++) o[(long long)c * n0 * jp] = d[c];
 }
 
+// x derivatives of the (F_x,c , v_c) pairs on the 2(order-1) closure planes
+// at each x face of a block, from the stage-start fields:
+// xcl[slot][q][j][k], slot 0..NB-1 planes 0..NB-1, slot NB+m plane n0-NB+m,
+// q = 2c (flux) or 2c+1 (velocity).  One thread per (j, k) and face: each of
+// the 3(order-1) planes the closure rows reach is loaded once.
+template <int ORDER>
+__global__ void __launch_bounds__(128) k_xcl3d(VolumeArgs<float> a, BlockDev B, float* __restrict__ xcl) {
+    constexpr int H = ORDER - 1, NB = 2 * H, NTB = 3 * H;
+    const int n0 = B.n[0], n1 = B.n[1], n2 = B.n[2];
+    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y;
+    const bool left = blockIdx.z == 0;
+    if (k >= n2 || j >= n1) return;
+    const float sg = left ? 1.f : -1.f;
+    const int cs = (int)a.L.cstride, s0 = (int)a.L.s0;
+    const int colbase = B.lo[0] * s0 + (B.lo[1] + j) * (int)a.L.s1 + (B.lo[2] + k);
+    float2 acc[NB][3];
+#pragma unroll
+    for (int r = 0; r < NB; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) acc[r][c] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int n = 0; n < NTB; n++) {
+        const int id = colbase + (left ? n : n0 - 1 - n) * s0;
+        float s[6], v[3], Fx[3];
+#pragma unroll
+        for (int c = 0; c < 6; c++) s[c] = __ldg(a.F + (3 + c) * cs + id);
+#pragma unroll
+        for (int c = 0; c < 3; c++) v[c] = __ldg(a.F + c * cs + id);
+        fluxes(__ldg(a.J + id), __ldg(a.M + id), __ldg(a.M + cs + id), __ldg(a.M + 2 * cs + id), s, Fx);
+        // closure row r+1 of the plane r from the face (left: plane r, right: plane n0-1-r)
+#pragma unroll
+        for (int r = 0; r < NB; r++) {
+            const float cf = sbp_coef<float>(ORDER, r + 1, n);
+#pragma unroll
+            for (int c = 0; c < 3; c++) acc[r][c] = fma2(cf, make_float2(Fx[c], v[c]), acc[r][c]);
+        }
+    }
+    const long long pl = (long long)n1 * n2;
+#pragma unroll
+    for (int r = 0; r < NB; r++) {
+        const int slot = left ? r : 2 * NB - 1 - r;   // right face: plane n0-1-r
+        float* o = xcl + (long long)slot * 6 * pl + (long long)j * n2 + k;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const float2 d = __fmul2_rn(make_float2(sg, sg), acc[r][c]);
+            o[2 * c * pl] = d.x;
+            o[(2 * c + 1) * pl] = d.y;
+        }
+    }
+}
+
 // choose the x chunk: the grid of tiles x chunks runs in whole waves of
 // `slots` resident CTAs; each chunk also pays about H planes of window set-up
 int pick_chunk(int n0, int tiles, int slots, int H) {
@@ -607,7 +656,8 @@ void launch_order(const VolumeArgs<float>& a, const BlockDev& b, int bi, const S
     if (b.bactive[4] || b.bactive[5])
         k_ksat3d<<<dim3((b.n[1] + 31) / 32, (b.n[0] + 3) / 4, 2), dim3(32, 4), 0, s>>>(a, b, sa, mh.ksat[bi],
                                                                                       mh.jp[bi]);
-    k_reg3d<ORDER><<<grid, NT, C::SMEM, s>>>(a, b, sa, chunk, status, mh.m, fsel, mh.kmap[bi]);
+    k_xcl3d<ORDER><<<dim3((b.n[2] + 31) / 32, (b.n[1] + 3) / 4, 2), dim3(32, 4), 0, s>>>(a, b, mh.xcl[bi]);
+    k_reg3d<ORDER><<<grid, NT, C::SMEM, s>>>(a, b, sa, chunk, status, mh.m, fsel, mh.kmap[bi], mh.xcl[bi]);
     launch_faces3d(a, b, sa, true, s);
 }
 
@@ -633,6 +683,7 @@ RegMapsHost* make_reg_maps(const Layout& L, const float* F0, const float* F1, co
         tma_encode(&h->m.JL, J, 3, d3, s4, d1);
         tma_encode(&h->m.DF, DF, 4, d4, s4, d9);
         h->ksat.assign(nblocks, nullptr);
+        h->xcl.assign(nblocks, nullptr);
         h->jp.assign(nblocks, 0);
         h->kmap.resize(nblocks);
         for (int b = 0; b < nblocks; b++) {
@@ -644,6 +695,12 @@ RegMapsHost* make_reg_maps(const Layout& L, const float* F0, const float* F1, co
                 throw std::runtime_error(std::string("CUDA error in cudaMalloc (k-face SAT buffer): ") +
                                          cudaGetErrorString(e));
             cudaMemset(h->ksat[b], 0, bytes);
+            // closure-plane x derivatives: up to 12 planes (order 4) x 6 values per node
+            const size_t xbytes = sizeof(float) * 12 * 6 * (size_t)blocks[b].n[1] * blocks[b].n[2];
+            const cudaError_t ex = cudaMalloc(&h->xcl[b], xbytes);
+            if (ex != cudaSuccess)
+                throw std::runtime_error(std::string("CUDA error in cudaMalloc (closure-plane buffer): ") +
+                                         cudaGetErrorString(ex));
             const cuuint64_t dk[3] = {(cuuint64_t)jp, (cuuint64_t)n0, 18};
             const cuuint64_t sk[2] = {(cuuint64_t)jp * 4, (cuuint64_t)n0 * jp * 4};
             const cuuint32_t bk[3] = {KBJ, 1, 9};
