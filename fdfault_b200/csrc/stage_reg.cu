@@ -97,11 +97,15 @@ struct RgCfg {
                          LF = CD + up32(9 * BOXD), LM = LF + up32(9 * BOXD), LJ = LM + up32(3 * BOXD),
                          KSW = up32(9 * KBJ), KS = LJ + up32(BOXD), SSZ = KS + 2 * KSW;
     static constexpr uint32_t BYTES = 4u * (19 * BOXC + 22 * BOXD), KBYTES = 4u * 9 * KBJ;
+    // window fill of a chunk: leading-plane boxes (13 components) of up to PR
+    // planes at a time in one stage
+    static constexpr uint32_t LBYTES = 4u * 13 * BOXD;
+    static constexpr int PR = SSZ / (13 * BOXD) < 3 ? SSZ / (13 * BOXD) : 3;
     static constexpr int TY = 3 * VH * TK, TZ = 3 * TJ * VW;   // float2
     static constexpr int WROWS = 2 * NB + 1;
     static constexpr int WTAB = ((WROWS * NTB + 3) / 4) * 4;
     static constexpr size_t SMEM =
-        sizeof(float) * 2 * SSZ + sizeof(float2) * (TY + TZ) + sizeof(float) * WTAB + 6 * sizeof(uint64_t);
+        sizeof(float) * 2 * SSZ + sizeof(float2) * (TY + TZ) + sizeof(float) * WTAB + 7 * sizeof(uint64_t);
 };
 
 template <int ORDER>
@@ -182,6 +186,7 @@ __global__ void __launch_bounds__(NT, 2)
     if (tid == 0) {
         bar_init(bar0);
         bar_init(bar1);
+        bar_init(saddr(bars + 6));   // window fill
         bar_init_count(barT, NWARP);
         bar_init_count(barR, NWARP);
         bar_init_count(barS, NWARP);
@@ -218,9 +223,12 @@ __global__ void __launch_bounds__(NT, 2)
         if (kf0) tma3(saddr(st + C::KS), &kmap, kjb, i, 0, bar);
         if (kf1) tma3(saddr(st + C::KS + C::KSW), &kmap, kjb, i, 9, bar);
     };
+    // a chunk that starts past the left closure rows fills its x window first
+    // through stage 1 (below), which takes plane ib+1 after that
+    const bool prefill = ib >= NB && ib < n0 - NB;
     if (tid == 0) {
         issue(ib, 0);
-        if (ib + 1 < ie) issue(ib + 1, 1);
+        if (ib + 1 < ie && !prefill) issue(ib + 1, 1);
     }
     int issued = min(ie, ib + 2);   // planes whose stage was issued (uniform over the CTA)
 
@@ -276,16 +284,6 @@ __global__ void __launch_bounds__(NT, 2)
         for (int c = 0; c < 3; c++) h.m[c] = __ldg(M + (3 + c) * cs + id);
         h.J = __ldg(Jg + id);
     };
-    // x flux and velocity of this thread's column at plane q, from global memory
-    auto direct = [&](int q, float Fx[3], float v[3]) {
-        const int id = colbase + q * s0;
-        float s[6];
-#pragma unroll
-        for (int c = 0; c < 6; c++) s[c] = __ldg(F + (3 + c) * cs + id);
-#pragma unroll
-        for (int c = 0; c < 3; c++) v[c] = __ldg(F + c * cs + id);
-        fluxes(__ldg(Jg + id), __ldg(M + id), __ldg(M + cs + id), __ldg(M + 2 * cs + id), s, Fx);
-    };
 
     float crho[3], sd[3];
 #pragma unroll
@@ -304,29 +302,57 @@ __global__ void __launch_bounds__(NT, 2)
         kface = B.defer[4 + kside] ? 2 : (B.bactive[4 + kside] ? 1 : 0);
     }
 
+    const int sod = tj * SWD + tk;   // this node in a staged rate or leading-plane component
     // x window: after the insert at plane i, w[m][c] holds the pair
     // (F_x,c , v_c) of plane i - H + m.  A chunk that starts past the left
-    // closure rows fills planes ib-H..ib+H-1 from global memory; the first
-    // chunk builds its window from the inserts.
+    // closure rows fills planes ib-H..ib+H-1 first: tensor copies of their
+    // leading-plane boxes, up to PR planes per round, through stage 1 (free
+    // until plane ib+1 is issued into it); the first chunk builds its window
+    // from the inserts.
     float2 w[W][3];
 #pragma unroll
     for (int m = 0; m < W; m++)
 #pragma unroll
         for (int c = 0; c < 3; c++) w[m][c] = make_float2(0.f, 0.f);
-    if (ib >= NB && ib < n0 - NB) {
+    if (prefill) {
+        constexpr int NPF = W - 1, PR = C::PR, PLN = 13 * BOXD;
+        float* pst = stg + C::SSZ;
+        const uint32_t barP = saddr(bars + 6);
 #pragma unroll
-        for (int m = 1; m < W; m++) {
-            float Fx[3], v[3];
-            direct(ib - H - 1 + m, Fx, v);
+        for (int t = 0; t < NPF; t++) {
+            const int p = t % PR, round = t / PR;
+            if (p == 0) {
+                const int np = min(PR, NPF - t);
+                if (tid == 0) {
+                    fence_proxy_async();
+                    bar_expect(barP, (uint32_t)np * C::LBYTES);
+                    for (int q = 0; q < np; q++) {
+                        const int ig = B.lo[0] + ib - H + t + q;
+                        float* d = pst + q * PLN;
+                        tma4(saddr(d), mFL, kg, jg, ig, 0, barP);
+                        tma4(saddr(d + 9 * BOXD), &maps.M3, kg, jg, ig, 0, barP);
+                        tma3(saddr(d + 12 * BOXD), &maps.JL, kg, jg, ig, barP);
+                    }
+                }
+                if (!bar_wait(barP, round & 1, wlim)) *abort_flag = 1;
+                // the issuing thread also sees the copies land before it reuses the space
+                if (tid == 0 && !bar_wait(barP, round & 1, TMA_DRAIN_LIMIT)) *abort_flag = 1;
+            }
+            const float* d = pst + p * PLN;
+            float s[6], Fx[3];
 #pragma unroll
-            for (int c = 0; c < 3; c++) w[m][c] = make_float2(Fx[c], v[c]);
+            for (int c = 0; c < 6; c++) s[c] = d[(3 + c) * BOXD + sod];
+            fluxes(d[12 * BOXD + sod], d[9 * BOXD + sod], d[10 * BOXD + sod], d[11 * BOXD + sod], s, Fx);
+#pragma unroll
+            for (int c = 0; c < 3; c++) w[t + 1][c] = make_float2(Fx[c], d[c * BOXD + sod]);
+            if (p == PR - 1 || t == NPF - 1) __syncthreads();   // round read before the space is refilled
         }
+        if (tid == 0 && ib + 1 < ie) issue(ib + 1, 1);
     }
     HaloNode hn;
     load_halo(ib, hn);
 
     const int so = tj * SWC + tk + KH;   // this node in a staged centre component
-    const int sod = tj * SWD + tk;       // ... in a staged rate or leading-plane component
     const int hso = hj * SWC + hk + KH;  // the k-halo node in a staged centre component
     for (int i = ib; i < ie; i++) {
         const int kk = i - ib;
