@@ -59,12 +59,12 @@ struct RegMaps {
 };
 
 struct RegMapsHost {
-    RegMaps m;
+    RegMaps m, me;   // boxes of the main tiles and of the narrower last-column tiles
     const float* F0;
-    // per block: k-face SAT increments [side][c][i][jp] and their tensor map
+    // per block: k-face SAT increments [side][c][i][jp] and their tensor maps (both tile heights)
     std::vector<float*> ksat;
     std::vector<int> jp;
-    std::vector<CUtensorMap> kmap;
+    std::vector<CUtensorMap> kmap, ekmap;
     // per block: x derivatives of the closure planes [slot][q][j][k] (see k_xcl3d)
     std::vector<float*> xcl;
     ~RegMapsHost() {
@@ -77,16 +77,21 @@ struct RegMapsHost {
 
 namespace {
 
-constexpr int TJ = 8, TK = 32, NT = TJ * TK;
+// tile shapes (j rows x k columns): the main tiles, and the narrower tile
+// that covers the last k columns of a block when n2 mod 32 is small (12 x 16,
+// 192 of the launch's 256 threads), so those columns are not computed twice
+constexpr int TJM = 8, TKM = 32, TJE = 12, TKE = 16;
+constexpr int NTL = 256;          // threads per CTA of the launch
 constexpr int KH = 4;             // halo columns staged on each side of the centre boxes (>= H, 16 bytes)
-constexpr int SWC = TK + 2 * KH;  // staged centre row, 40 floats
-constexpr int SWD = TK;           // staged row of the rate register and the leading plane
 
 constexpr int up32(int n) { return (n + 31) / 32 * 32; }   // every box on a 128-byte boundary
-constexpr int KBJ = TJ + 4;   // staged k-face row: 16-byte boundary at or below the tile's first j
 
-template <int ORDER>
+template <int ORDER, int TJ_ = TJM, int TK_ = TKM>
 struct RgCfg {
+    static constexpr int TJ = TJ_, TK = TK_, NT = TJ * TK;
+    static constexpr int SWC = TK + 2 * KH;  // staged centre row
+    static constexpr int SWD = TK;           // staged row of the rate register and the leading plane
+    static constexpr int KBJ = TJ + 4;       // staged k-face row: 16-byte boundary at or below the first j
     static constexpr int H = ORDER - 1, NB = 2 * H, NTB = 3 * H, W = 2 * H + 1;
     static constexpr int VH = TJ + 2 * H, VW = TK + 2 * H;
     static constexpr int BOXC = TJ * SWC, BOXD = TJ * SWD;   // floats of one staged component
@@ -106,6 +111,19 @@ struct RgCfg {
     static constexpr int WTAB = ((WROWS * NTB + 3) / 4) * 4;
     static constexpr size_t SMEM =
         sizeof(float) * 2 * SSZ + sizeof(float2) * (TY + TZ) + sizeof(float) * WTAB + 7 * sizeof(uint64_t);
+};
+// dynamic shared memory of a launch: the larger of the two shapes
+template <int ORDER>
+constexpr size_t reg_smem() {
+    return RgCfg<ORDER, TJM, TKM>::SMEM > RgCfg<ORDER, TJE, TKE>::SMEM ? RgCfg<ORDER, TJM, TKM>::SMEM
+                                                                         : RgCfg<ORDER, TJE, TKE>::SMEM;
+}
+
+// one CTA's tile: origin, tile indices, the last tiles in k and j, and the k
+// columns it owns away from the closure rows
+struct RegTile {
+    int k0, j0, bx, by, kown0, kown1;
+    bool lastk, lastj;
 };
 
 template <int ORDER>
@@ -129,14 +147,14 @@ struct HaloNode {
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
 __device__ __forceinline__ float2 fma2(float a, float2 x, float2 acc) { return __ffma2_rn(make_float2(a, a), x, acc); }
 
-template <int ORDER>
-__global__ void __launch_bounds__(NT, 2)
-    k_reg3d(VolumeArgs<float> a, BlockDev B, StageArgs sa, int chunk, int* status,
-            const __grid_constant__ RegMaps maps, int fsel, const __grid_constant__ CUtensorMap kmap,
-            const float* __restrict__ xcl) {
-    using C = RgCfg<ORDER>;
+template <int ORDER, int TJ, int TK>
+__device__ __forceinline__ void reg_march(const VolumeArgs<float>& a, const BlockDev& B, const StageArgs& sa,
+                                          int chunk, int* status, const RegMaps& maps, int fsel,
+                                          const CUtensorMap& kmap, const float* __restrict__ xcl, const RegTile& T) {
+    using C = RgCfg<ORDER, TJ, TK>;
     constexpr int H = C::H, NB = C::NB, NTB = C::NTB, W = C::W, VH = C::VH, VW = C::VW, BOXC = C::BOXC,
                   BOXD = C::BOXD;
+    constexpr int NT = C::NT, SWC = C::SWC, SWD = C::SWD, KBJ = C::KBJ;
     extern __shared__ __align__(128) float smem[];
     float* stg = smem;                                            // two stages of C::SSZ floats
     float2* ty = reinterpret_cast<float2*>(smem + 2 * C::SSZ);   // [3][VH][TK]  (F_y,c , v_c)
@@ -147,17 +165,16 @@ __global__ void __launch_bounds__(NT, 2)
     const Layout& L = a.L;
     const int cs = (int)L.cstride;
     const int n0 = B.n[0], n1 = B.n[1], n2 = B.n[2];
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x;   // threads from NT on (the narrower tile) only share the set-up barriers
     const int tk = tid % TK, tj = tid / TK;
     // tiles and ownership as in stage_fast.cu: the last tile in j ends on the
     // block face, the last tile in k at or up to 3 columns past it (its first
     // column on a 4-column boundary); each owns the closure rows near its face
-    const bool lastk = blockIdx.x == gridDim.x - 1, lastj = blockIdx.y == gridDim.y - 1;
-    const int k0 = lastk ? ((n2 - TK + 3) & ~3) : blockIdx.x * TK;
-    const int j0 = lastj ? n1 - TJ : blockIdx.y * TJ;
+    const bool lastk = T.lastk, lastj = T.lastj;
+    const int k0 = T.k0, j0 = T.j0;
     const int k = k0 + tk, j = j0 + tj;
-    const bool ownk = (k >= n2) ? false : (k >= n2 - NB) ? lastk : (k / TK == (int)blockIdx.x);
-    const bool ownj = (j >= n1 - NB) ? lastj : (j / TJ == (int)blockIdx.y);
+    const bool ownk = (k >= n2) ? false : (k >= n2 - NB) ? lastk : (k >= T.kown0 && k < T.kown1);
+    const bool ownj = (j >= n1 - NB) ? lastj : (j / TJ == T.by);
     const bool owner = ownk && ownj;
     const int ib = blockIdx.z * chunk;
     const int ie = min(n0, ib + chunk);
@@ -178,9 +195,9 @@ __global__ void __launch_bounds__(NT, 2)
     volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 5);
     const int lane = tid & 31;
 
-    const bool kedge = (blockIdx.x == 0) || lastk;
+    const bool kedge = (T.bx == 0) || lastk;
     // k faces whose SAT increments this tile stages (outer faces with a SAT)
-    const bool kf0 = (blockIdx.x == 0) && B.bactive[4], kf1 = lastk && B.bactive[5];
+    const bool kf0 = (T.bx == 0) && B.bactive[4], kf1 = lastk && B.bactive[5];
     const int kjb = j0 & ~3;   // k-face box origin in j (block coordinates)
     const uint32_t bytes = C::BYTES + (kf0 ? C::KBYTES : 0u) + (kf1 ? C::KBYTES : 0u);
     if (tid == 0) {
@@ -338,17 +355,20 @@ __global__ void __launch_bounds__(NT, 2)
                 // the issuing thread also sees the copies land before it reuses the space
                 if (tid == 0 && !bar_wait(barP, round & 1, TMA_DRAIN_LIMIT)) *abort_flag = 1;
             }
-            const float* d = pst + p * PLN;
-            float s[6], Fx[3];
+            if (tid < NT) {
+                const float* d = pst + p * PLN;
+                float s[6], Fx[3];
 #pragma unroll
-            for (int c = 0; c < 6; c++) s[c] = d[(3 + c) * BOXD + sod];
-            fluxes(d[12 * BOXD + sod], d[9 * BOXD + sod], d[10 * BOXD + sod], d[11 * BOXD + sod], s, Fx);
+                for (int c = 0; c < 6; c++) s[c] = d[(3 + c) * BOXD + sod];
+                fluxes(d[12 * BOXD + sod], d[9 * BOXD + sod], d[10 * BOXD + sod], d[11 * BOXD + sod], s, Fx);
 #pragma unroll
-            for (int c = 0; c < 3; c++) w[t + 1][c] = make_float2(Fx[c], d[c * BOXD + sod]);
+                for (int c = 0; c < 3; c++) w[t + 1][c] = make_float2(Fx[c], d[c * BOXD + sod]);
+            }
             if (p == PR - 1 || t == NPF - 1) __syncthreads();   // round read before the space is refilled
         }
         if (tid == 0 && ib + 1 < ie) issue(ib + 1, 1);
     }
+    if (tid >= NT) return;   // no part in the march (its barriers count NT / 32 warps)
     HaloNode hn;
     load_halo(ib, hn);
 
@@ -563,6 +583,42 @@ __global__ void __launch_bounds__(NT, 2)
     }
 }
 
+// One launch per block and stage: blockIdx.x < tkm are the main tiles along k
+// (8 x 32); with `edge` set, blockIdx.x == tkm is the column of narrower tiles
+// (12 x 16) over the last k columns, which owns k >= 32 tkm.
+template <int ORDER>
+__global__ void __launch_bounds__(NTL, 2)
+    k_reg3d(VolumeArgs<float> a, BlockDev B, StageArgs sa, int chunk, int* status, int tkm, int edge,
+            const __grid_constant__ RegMaps maps, const __grid_constant__ RegMaps emaps, int fsel,
+            const __grid_constant__ CUtensorMap kmap, const __grid_constant__ CUtensorMap ekmap,
+            const float* __restrict__ xcl) {
+    const int n1 = B.n[1], n2 = B.n[2];
+    RegTile T;
+    T.bx = blockIdx.x;
+    T.by = blockIdx.y;
+    if (edge && T.bx == tkm) {
+        const int tje = (n1 + TJE - 1) / TJE;
+        if (T.by >= tje) return;
+        T.lastk = true;
+        T.lastj = T.by == tje - 1;
+        T.k0 = (n2 - TKE + 3) & ~3;
+        T.j0 = T.lastj ? n1 - TJE : T.by * TJE;
+        T.kown0 = tkm * TKM;
+        T.kown1 = n2;
+        reg_march<ORDER, TJE, TKE>(a, B, sa, chunk, status, emaps, fsel, ekmap, xcl, T);
+    } else {
+        const int tjm = (n1 + TJM - 1) / TJM;
+        if (T.by >= tjm) return;
+        T.lastk = !edge && T.bx == tkm - 1;
+        T.lastj = T.by == tjm - 1;
+        T.k0 = T.lastk ? ((n2 - TKM + 3) & ~3) : T.bx * TKM;
+        T.j0 = T.lastj ? n1 - TJM : T.by * TJM;
+        T.kown0 = T.bx * TKM;
+        T.kown1 = T.kown0 + TKM;
+        reg_march<ORDER, TJM, TKM>(a, B, sa, chunk, status, maps, fsel, kmap, xcl, T);
+    }
+}
+
 // SAT increments of the two k faces of a block from the stage-start fields:
 // ks[side][c][i][jp] = the change the face's SAT makes to the rate of node
 // (i, j, k = 0 or n2-1).  One thread per face node, threads along j.
@@ -659,7 +715,8 @@ int pick_chunk(int n0, int tiles, int slots, int H) {
 template <int ORDER>
 void launch_order(const VolumeArgs<float>& a, const BlockDev& b, int bi, const StageArgs& sa, int* status,
                   const RegMapsHost& mh, cudaStream_t s) {
-    using C = RgCfg<ORDER>;
+    constexpr size_t SMEM = reg_smem<ORDER>();
+    constexpr int NB = 2 * (ORDER - 1);
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     // the shared-memory opt-in is a per-device function attribute: set it once per device
@@ -667,23 +724,30 @@ void launch_order(const VolumeArgs<float>& a, const BlockDev& b, int bi, const S
     static int occ[32] = {0};
     const unsigned bit = 1u << (dev & 31);
     if (!(configured.load() & bit)) {
-        cudaFuncSetAttribute(k_reg3d<ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+        cudaFuncSetAttribute(k_reg3d<ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
         int o = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_reg3d<ORDER>, NT, C::SMEM);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_reg3d<ORDER>, NTL, SMEM);
         occ[dev & 31] = o > 0 ? o : 1;
         configured.fetch_or(bit);
     }
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const int tk = (b.n[2] + TK - 1) / TK, tj = (b.n[1] + TJ - 1) / TJ;
-    const int chunk = pick_chunk(b.n[0], tk * tj, occ[dev & 31] * nsm, ORDER - 1);
+    // the narrower tiles take the last k columns when n2 mod 32 leaves between
+    // NB (its closure rows) and 16 columns
+    const int rem = b.n[2] % TKM;
+    const int edge = (rem >= NB && rem <= TKE && b.n[2] > TKM && b.n[1] >= TJE) ? 1 : 0;
+    const int tkm = edge ? b.n[2] / TKM : (b.n[2] + TKM - 1) / TKM;
+    const int tjm = (b.n[1] + TJM - 1) / TJM, tje = (b.n[1] + TJE - 1) / TJE;
+    const int tiles = tkm * tjm + (edge ? tje : 0);
+    const int chunk = pick_chunk(b.n[0], tiles, occ[dev & 31] * nsm, ORDER - 1);
     const int chunks = (b.n[0] + chunk - 1) / chunk;
-    dim3 grid(tk, tj, chunks);
+    dim3 grid(tkm + edge, edge ? (tjm > tje ? tjm : tje) : tjm, chunks);
     const int fsel = (a.F == mh.F0) ? 0 : 1;
     if (b.bactive[4] || b.bactive[5])
         k_ksat3d<<<dim3((b.n[1] + 31) / 32, (b.n[0] + 3) / 4, 2), dim3(32, 4), 0, s>>>(a, b, sa, mh.ksat[bi],
                                                                                       mh.jp[bi]);
     k_xcl3d<ORDER><<<dim3((b.n[2] + 31) / 32, (b.n[1] + 3) / 4, 2), dim3(32, 4), 0, s>>>(a, b, mh.xcl[bi]);
-    k_reg3d<ORDER><<<grid, NT, C::SMEM, s>>>(a, b, sa, chunk, status, mh.m, fsel, mh.kmap[bi], mh.xcl[bi]);
+    k_reg3d<ORDER><<<grid, NTL, SMEM, s>>>(a, b, sa, chunk, status, tkm, edge, mh.m, mh.me, fsel, mh.kmap[bi],
+                                           mh.ekmap[bi], mh.xcl[bi]);
     launch_faces3d(a, b, sa, true, s);
 }
 
@@ -696,22 +760,29 @@ RegMapsHost* make_reg_maps(const Layout& L, const float* F0, const float* F1, co
     const cuuint64_t d4[4] = {(cuuint64_t)L.s1, (cuuint64_t)L.nx[1], (cuuint64_t)L.nx[0], 9};
     const cuuint64_t s4[3] = {(cuuint64_t)L.s1 * 4, (cuuint64_t)L.s0 * 4, (cuuint64_t)L.cstride * 4};
     const cuuint64_t d3[3] = {(cuuint64_t)L.s1, (cuuint64_t)L.nx[1], (cuuint64_t)L.nx[0]};
-    const cuuint32_t c9[4] = {SWC, TJ, 1, 9}, c1[3] = {SWC, TJ, 1};
-    const cuuint32_t d9[4] = {SWD, TJ, 1, 9}, d3b[4] = {SWD, TJ, 1, 3}, d1[3] = {SWD, TJ, 1};
+    // one set of maps per tile shape (box tj rows; centre rows tk + 2 KH wide, others tk)
+    auto encode = [&](RegMaps& m, cuuint32_t tj, cuuint32_t tk) {
+        const cuuint32_t swc = tk + 2 * KH;
+        const cuuint32_t c9[4] = {swc, tj, 1, 9}, c1[3] = {swc, tj, 1};
+        const cuuint32_t d9[4] = {tk, tj, 1, 9}, d3b[4] = {tk, tj, 1, 3}, d1[3] = {tk, tj, 1};
+        tma_encode(&m.F[0], F0, 4, d4, s4, c9);
+        tma_encode(&m.F[1], F1, 4, d4, s4, c9);
+        tma_encode(&m.M9, M, 4, d4, s4, c9);
+        tma_encode(&m.J, J, 3, d3, s4, c1);
+        tma_encode(&m.FL[0], F0, 4, d4, s4, d9);
+        tma_encode(&m.FL[1], F1, 4, d4, s4, d9);
+        tma_encode(&m.M3, M, 4, d4, s4, d3b);
+        tma_encode(&m.JL, J, 3, d3, s4, d1);
+        tma_encode(&m.DF, DF, 4, d4, s4, d9);
+    };
     try {
-        tma_encode(&h->m.F[0], F0, 4, d4, s4, c9);
-        tma_encode(&h->m.F[1], F1, 4, d4, s4, c9);
-        tma_encode(&h->m.M9, M, 4, d4, s4, c9);
-        tma_encode(&h->m.J, J, 3, d3, s4, c1);
-        tma_encode(&h->m.FL[0], F0, 4, d4, s4, d9);
-        tma_encode(&h->m.FL[1], F1, 4, d4, s4, d9);
-        tma_encode(&h->m.M3, M, 4, d4, s4, d3b);
-        tma_encode(&h->m.JL, J, 3, d3, s4, d1);
-        tma_encode(&h->m.DF, DF, 4, d4, s4, d9);
+        encode(h->m, TJM, TKM);
+        encode(h->me, TJE, TKE);
         h->ksat.assign(nblocks, nullptr);
         h->xcl.assign(nblocks, nullptr);
         h->jp.assign(nblocks, 0);
         h->kmap.resize(nblocks);
+        h->ekmap.resize(nblocks);
         for (int b = 0; b < nblocks; b++) {
             const int n0 = blocks[b].n[0], jp = (blocks[b].n[1] + 3) / 4 * 4;
             h->jp[b] = jp;
@@ -729,8 +800,9 @@ RegMapsHost* make_reg_maps(const Layout& L, const float* F0, const float* F1, co
                                          cudaGetErrorString(ex));
             const cuuint64_t dk[3] = {(cuuint64_t)jp, (cuuint64_t)n0, 18};
             const cuuint64_t sk[2] = {(cuuint64_t)jp * 4, (cuuint64_t)n0 * jp * 4};
-            const cuuint32_t bk[3] = {KBJ, 1, 9};
+            const cuuint32_t bk[3] = {TJM + 4, 1, 9}, bke[3] = {TJE + 4, 1, 9};
             tma_encode(&h->kmap[b], h->ksat[b], 3, dk, sk, bk);
+            tma_encode(&h->ekmap[b], h->ksat[b], 3, dk, sk, bke);
         }
     } catch (...) {
         delete h;
@@ -745,7 +817,7 @@ bool reg3d_supported(const Layout& L, const BlockDev& b, int order) {
     if (b.mat) return false;   // one material per block
     if (L.ndim != 3 || L.nfields != 9) return false;
     if (order < 2 || order > 4) return false;
-    if (b.n[1] < TJ || b.n[2] < TK) return false;
+    if (b.n[1] < TJM || b.n[2] < TKM) return false;
     if (b.n[0] < 4 * order - 3) return false;
     if (L.cstride * 9 >= (1LL << 31)) return false;   // 32-bit element offsets
     if (L.s1 % 4 != 0 || L.s0 % 4 != 0 || L.cstride % 4 != 0) return false;   // 16-byte row starts
