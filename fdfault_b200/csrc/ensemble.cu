@@ -122,6 +122,7 @@ Ensemble::Ensemble(const std::vector<std::string>& infiles, int device) : device
         Solver& s = *members_[m];
         if (s.nstages_ != nstages_) throw std::invalid_argument("ensemble members must share the Runge-Kutta order");
         if (s.P_.plastic()) throw std::invalid_argument("ensemble members must be elastic");
+        if (s.mat_) throw std::invalid_argument("ensemble members must have one material per block");
         if ((int)s.blocks_.size() > ENS_MAX_BLOCKS || s.ifaces_.size() > 2)
             throw std::invalid_argument("ensemble member has too many blocks or interfaces");
         for (const auto& I : s.ifaces_)

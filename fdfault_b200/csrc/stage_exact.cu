@@ -21,9 +21,9 @@ namespace fdf {
 
 namespace {
 
-template <typename T, int NDIM, int MODE>
+template <typename T, int NDIM, int MODE, bool HET>
 __global__ void __launch_bounds__(128) k_volume_exact(VolumeArgs<T> a, BlockDev B, StageArgs sa) {
-    volume_node<T, NDIM, MODE>(a, B, sa, blockIdx.x * (long long)blockDim.x + threadIdx.x);
+    volume_node<T, NDIM, MODE, HET>(a, B, sa, blockIdx.x * (long long)blockDim.x + threadIdx.x);
 }
 
 // Every block of a problem in one launch: thread t takes node t - start[b] of
@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(128) k_volume_exact(VolumeArgs<T> a, BlockDev 
 // per-block launch (the block table is read from device memory).  Small
 // problems, whose per-block launches each fill a fraction of one wave, then
 // overlap their blocks.
-template <typename T, int NDIM, int MODE>
+template <typename T, int NDIM, int MODE, bool HET>
 __global__ void __launch_bounds__(128) k_volume_exact_all(VolumeArgs<T> a, const BlockDev* __restrict__ blks,
                                                           BlockRanges r, StageArgs sa) {
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -44,7 +44,7 @@ __global__ void __launch_bounds__(128) k_volume_exact_all(VolumeArgs<T> a, const
             b = q;
             s = r.start[q];
         }
-    volume_node<T, NDIM, MODE>(a, blks[b], sa, t - s);
+    volume_node<T, NDIM, MODE, HET>(a, blks[b], sa, t - s);
 }
 
 }  // namespace
@@ -53,12 +53,20 @@ template <typename T>
 void launch_volume_exact(const VolumeArgs<T>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s) {
     long long nn = (long long)b.n[0] * b.n[1] * b.n[2];
     unsigned grid = (unsigned)((nn + 127) / 128);
-    if (a.L.ndim == 3)
-        k_volume_exact<T, 3, 2><<<grid, 128, 0, s>>>(a, b, sa);
-    else if (a.L.mode == 2)
-        k_volume_exact<T, 2, 2><<<grid, 128, 0, s>>>(a, b, sa);
-    else
-        k_volume_exact<T, 2, 3><<<grid, 128, 0, s>>>(a, b, sa);
+    // heterogeneous material: modes II and 3D (mode III is rejected at input)
+    if (a.L.ndim == 3) {
+        if (b.mat)
+            k_volume_exact<T, 3, 2, true><<<grid, 128, 0, s>>>(a, b, sa);
+        else
+            k_volume_exact<T, 3, 2, false><<<grid, 128, 0, s>>>(a, b, sa);
+    } else if (a.L.mode == 2) {
+        if (b.mat)
+            k_volume_exact<T, 2, 2, true><<<grid, 128, 0, s>>>(a, b, sa);
+        else
+            k_volume_exact<T, 2, 2, false><<<grid, 128, 0, s>>>(a, b, sa);
+    } else {
+        k_volume_exact<T, 2, 3, false><<<grid, 128, 0, s>>>(a, b, sa);
+    }
 }
 
 template <typename T>
@@ -72,12 +80,20 @@ void launch_volume_exact_all(const VolumeArgs<T>& a, const BlockDev* blks_dev, c
     }
     r.start[FDF_ALLB_MAX] = n;   // ranges of absent blocks are empty and never selected
     const unsigned grid = (unsigned)((n + 127) / 128);
-    if (a.L.ndim == 3)
-        k_volume_exact_all<T, 3, 2><<<grid, 128, 0, s>>>(a, blks_dev, r, sa);
-    else if (a.L.mode == 2)
-        k_volume_exact_all<T, 2, 2><<<grid, 128, 0, s>>>(a, blks_dev, r, sa);
-    else
-        k_volume_exact_all<T, 2, 3><<<grid, 128, 0, s>>>(a, blks_dev, r, sa);
+    const bool het = nb > 0 && blks[0].mat != nullptr;   // one material array for all blocks
+    if (a.L.ndim == 3) {
+        if (het)
+            k_volume_exact_all<T, 3, 2, true><<<grid, 128, 0, s>>>(a, blks_dev, r, sa);
+        else
+            k_volume_exact_all<T, 3, 2, false><<<grid, 128, 0, s>>>(a, blks_dev, r, sa);
+    } else if (a.L.mode == 2) {
+        if (het)
+            k_volume_exact_all<T, 2, 2, true><<<grid, 128, 0, s>>>(a, blks_dev, r, sa);
+        else
+            k_volume_exact_all<T, 2, 2, false><<<grid, 128, 0, s>>>(a, blks_dev, r, sa);
+    } else {
+        k_volume_exact_all<T, 2, 3, false><<<grid, 128, 0, s>>>(a, blks_dev, r, sa);
+    }
 }
 
 template void launch_volume_exact_all<double>(const VolumeArgs<double>&, const BlockDev*, const BlockDev*, int,

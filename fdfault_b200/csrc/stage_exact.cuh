@@ -16,7 +16,9 @@
 
 namespace fdf {
 
-template <typename T, int NDIM, int MODE>
+// HET: the problem has a heterogeneous material (per-node moduli); kept out
+// of the common instantiation, whose register budget it would raise
+template <typename T, int NDIM, int MODE, bool HET = false>
 __device__ __forceinline__ void volume_node(const VolumeArgs<T>& a, const BlockDev& B, const StageArgs& sa,
                                             long long t) {
     const Layout& L = a.L;
@@ -44,7 +46,7 @@ __device__ __forceinline__ void volume_node(const VolumeArgs<T>& a, const BlockD
     const T jc = J[id];
     for (int d = 0; d < NDIM; d++) {
         T invrho = (T)B.coef[d][0], g2lam = (T)B.coef[d][1], g = (T)B.coef[d][2], lambda = (T)B.coef[d][3];
-        if (B.mat) {   // per-node material (block.cpp:1061-1065 and the other passes)
+        if (HET) {   // per-node material (block.cpp:1061-1065 and the other passes)
             const double rho = B.mat[id], lm = B.mat[cs + id], gg = B.mat[2 * cs + id];
             invrho = (T)(sa.dt / rho / B.dx[d]);
             g2lam = (T)(sa.dt * (2. * gg + lm) / B.dx[d]);
@@ -129,7 +131,7 @@ __device__ __forceinline__ void volume_node(const VolumeArgs<T>& a, const BlockD
     }
     if (NDIM == 2 && MODE == 2 && plastic) {
         T nu = (T)B.nu;
-        if (B.mat) {
+        if (HET) {
             // block.cpp:1289-1291 reads lambda at the node and, as its second
             // term, the material array one x row further on (mat[nxd[1] + index]):
             // rho of node (i+1, j), or past the last row lambda of (0, j)
@@ -166,7 +168,7 @@ __device__ __forceinline__ void volume_node(const VolumeArgs<T>& a, const BlockD
         T fv[9];
 #pragma unroll
         for (int q = 0; q < NF; q++) fv[q] = F[q * cs + id];
-        boundary_sat<T, NDIM, MODE>(B, f, fa, fb, (T)sa.dt, fv, df, plastic, id);
+        boundary_sat<T, NDIM, MODE>(B, f, fa, fb, (T)sa.dt, fv, df, plastic, HET ? id : -1);
     }
     (void)onface;
     for (int q = 0; q < nfd; q++) a.DF[q * cs + id] = df[q];
