@@ -152,7 +152,8 @@ int fdf_use_fast_kernel(fdf_handle* h, int on, int* active);
  * every plane of a tile staged by TMA tensor copies; plastic or dissipative
  * stages run kind 1; for 2D problems it selects the tiled 2D kernel like
  * kind 1).  active = the kind that will run (0 where the chosen one does not
- * apply to the problem; FP64 problems always run kind 0). */
+ * apply to the problem: FP64 problems and problems with a heterogeneous
+ * material file always run kind 0). */
 int fdf_set_volume_kernel(fdf_handle* h, int kind, int* active);
 
 /* Polls of each bounded wait for staged data in the TMA-staged volume kernels
