@@ -86,10 +86,16 @@ void free_reg_maps(RegMapsHost* h);
 void launch_volume_reg3d(const VolumeArgs<float>& a, const BlockDev& b, int bi, const StageArgs& sa, int* status,
                          const RegMapsHost* maps, cudaStream_t s);
 bool reg3d_supported(const Layout& L, const BlockDev& b, int order);
-// outer SATs and RK update of the face nodes of a 3D block (elastic), after a
-// marching kernel wrote their rate without the SAT (kdone: the k-face SATs are
-// already in the rate and nodes on k faces only are finished)
-void launch_faces3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, bool kdone, cudaStream_t s);
+// outer SATs and RK update of the face nodes of a 3D block, after a marching
+// kernel wrote their rate without the SAT (kdone: the k-face SATs are already
+// in the rate and nodes on k faces only are finished); plastic: the last
+// stage's return map too
+void launch_faces3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, bool kdone, bool plastic,
+                    cudaStream_t s);
+// return map of a 3D block's nodes off the x and y faces after a marching
+// kernel (kall: nodes on k faces included, except interface faces)
+void launch_return_map3(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, bool kall,
+                        cudaStream_t s);
 
 // interface kernels
 template <typename T>

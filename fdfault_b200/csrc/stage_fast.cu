@@ -499,14 +499,19 @@ __global__ void __launch_bounds__(128) k_faces3d(VolumeArgs<float> a, BlockDev B
 }
 
 // Drucker-Prager return map (finish_node on the last stage) of the interior
-// nodes of a block, after k_fast3d wrote their updated fields: face nodes were
-// finished by k_faces3d and fault nodes by the interface kernel.  Kept out of
-// the marching kernel, whose register budget the FP64 return map would exceed.
-__global__ void __launch_bounds__(256) k_return_map3(VolumeArgs<float> a, BlockDev B, StageArgs sa) {
-    const int n1i = B.n[1] - 2, n2i = B.n[2] - 2;
+// nodes of a block, after a marching kernel wrote their updated fields: face
+// nodes were finished by k_faces3d and fault nodes by the interface kernel.
+// With kall the nodes on the k faces are included (the register-window kernel
+// finishes them itself), except on k faces that an interface finishes.  Kept
+// out of the marching kernels, whose register budget the FP64 return map
+// would exceed.
+__global__ void __launch_bounds__(256) k_return_map3(VolumeArgs<float> a, BlockDev B, StageArgs sa, int kall) {
+    const int n1i = B.n[1] - 2, n2i = kall ? B.n[2] : B.n[2] - 2;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)(B.n[0] - 2) * n1i * n2i) return;
-    const int k = 1 + (int)(t % n2i), j = 1 + (int)((t / n2i) % n1i), i = 1 + (int)(t / ((long long)n2i * n1i));
+    const int k = (kall ? 0 : 1) + (int)(t % n2i), j = 1 + (int)((t / n2i) % n1i),
+              i = 1 + (int)(t / ((long long)n2i * n1i));
+    if ((k == 0 && B.defer[4]) || (k == B.n[2] - 1 && B.defer[5])) return;
     const Layout& L = a.L;
     const long long cs = L.cstride;
     const long long id = node_index(L, B.lo[0] + i, B.lo[1] + j, B.lo[2] + k);
@@ -543,10 +548,7 @@ void launch_order(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs
     k_fast3d<ORDER><<<grid, NT, C::SMEM, s>>>(a, b, sa, chunk);
     const int nbmax = b.n[2] > b.n[1] ? b.n[2] : b.n[1], namax = b.n[0] > b.n[1] ? b.n[0] : b.n[1];
     k_faces3d<PLASTIC><<<dim3((nbmax + 31) / 32, (namax + 3) / 4, 6), dim3(32, 4), 0, s>>>(a, b, sa, 0);
-    if (PLASTIC && sa.last) {
-        const long long nin = (long long)(b.n[0] - 2) * (b.n[1] - 2) * (b.n[2] - 2);
-        k_return_map3<<<(unsigned)((nin + 255) / 256), 256, 0, s>>>(a, b, sa);
-    }
+    if (PLASTIC && sa.last) launch_return_map3(a, b, sa, false, s);
 }
 
 template <bool PLASTIC>
@@ -570,10 +572,20 @@ bool fast3d_supported(const Layout& L, const BlockDev& b, int order) {
     return true;
 }
 
-void launch_faces3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, bool kdone, cudaStream_t s) {
+void launch_faces3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, bool kdone, bool plastic,
+                    cudaStream_t s) {
     const int nbmax = b.n[2] > b.n[1] ? b.n[2] : b.n[1], namax = b.n[0] > b.n[1] ? b.n[0] : b.n[1];
-    k_faces3d<false><<<dim3((nbmax + 31) / 32, (namax + 3) / 4, kdone ? 4 : 6), dim3(32, 4), 0, s>>>(a, b, sa,
-                                                                                                   kdone ? 1 : 0);
+    const dim3 grid((nbmax + 31) / 32, (namax + 3) / 4, kdone ? 4 : 6);
+    if (plastic)
+        k_faces3d<true><<<grid, dim3(32, 4), 0, s>>>(a, b, sa, kdone ? 1 : 0);
+    else
+        k_faces3d<false><<<grid, dim3(32, 4), 0, s>>>(a, b, sa, kdone ? 1 : 0);
+}
+
+void launch_return_map3(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, bool kall,
+                        cudaStream_t s) {
+    const long long nin = (long long)(b.n[0] - 2) * (b.n[1] - 2) * (kall ? b.n[2] : b.n[2] - 2);
+    k_return_map3<<<(unsigned)((nin + 255) / 256), 256, 0, s>>>(a, b, sa, kall ? 1 : 0);
 }
 
 void launch_volume_fast3d(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s) {

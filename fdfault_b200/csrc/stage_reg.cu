@@ -748,7 +748,10 @@ void launch_order(const VolumeArgs<float>& a, const BlockDev& b, int bi, const S
     k_xcl3d<ORDER><<<dim3((b.n[2] + 31) / 32, (b.n[1] + 3) / 4, 2), dim3(32, 4), 0, s>>>(a, b, mh.xcl[bi]);
     k_reg3d<ORDER><<<grid, NTL, SMEM, s>>>(a, b, sa, chunk, status, tkm, edge, mh.m, mh.me, fsel, mh.kmap[bi],
                                            mh.ekmap[bi], mh.xcl[bi]);
-    launch_faces3d(a, b, sa, true, s);
+    // plasticity: face nodes get the return map in the face-node kernel, the
+    // others (k-face nodes included, finished by the march) in their own pass
+    launch_faces3d(a, b, sa, true, sa.plastic != 0, s);
+    if (sa.plastic && sa.last) launch_return_map3(a, b, sa, true, s);
 }
 
 }  // namespace
@@ -827,7 +830,7 @@ bool reg3d_supported(const Layout& L, const BlockDev& b, int order) {
 
 void launch_volume_reg3d(const VolumeArgs<float>& a, const BlockDev& b, int bi, const StageArgs& sa, int* status,
                          const RegMapsHost* maps, cudaStream_t s) {
-    if (a.cdiss > 0. || sa.plastic) {   // dissipation / plasticity: the tiled kernel of stage_fast.cu
+    if (a.cdiss > 0.) {   // artificial dissipation: the tiled kernel of stage_fast.cu
         launch_volume_fast3d(a, b, sa, s);
         return;
     }

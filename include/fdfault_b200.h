@@ -149,8 +149,8 @@ int fdf_use_fast_kernel(fdf_handle* h, int on, int* active);
  * blocks at least 32 nodes wide in y), 2 staged (3D only: planes brought into
  * shared memory by TMA tensor copies), 3 register window (the default: 3D
  * blocks of the same sizes as kind 1, the x stencil window in registers and
- * every plane of a tile staged by TMA tensor copies; plastic or dissipative
- * stages run kind 1; for 2D problems it selects the tiled 2D kernel like
+ * every plane of a tile staged by TMA tensor copies; plastic stages add the
+ * return map in separate passes, dissipative stages run kind 0; for 2D problems it selects the tiled 2D kernel like
  * kind 1).  active = the kind that will run (0 where the chosen one does not
  * apply to the problem: FP64 problems and problems with a heterogeneous
  * material file always run kind 0). */
