@@ -233,6 +233,11 @@ int fdf_get_fault(fdf_handle* h, int iface, int which, double* out) {
     return guarded(h, [&](fdf::Solver& s) { s.get_fault(iface, which, out); });
 }
 
+int fdf_get_fault_async(fdf_handle* h, int iface, int which, double* out) {
+    if (!out) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { s.get_fault_async(iface, which, out); });
+}
+
 int fdf_set_fault(fdf_handle* h, int iface, int which, const double* in) {
     if (!in) return FDF_ERR_ARG;
     return guarded(h, [&](fdf::Solver& s) { s.set_fault(iface, which, in); });

@@ -1029,16 +1029,16 @@ void Solver::do_rk_stage(double dt, int stage, double t) {
 
 void Solver::step(int nsteps) {
     check_plastic_rule();
-    // whole pairs of steps replay the captured graph when nothing on the host
-    // has to happen between steps (no output units, no per-launch profiling)
-    if (graphs_ && !out_ && !profile_ && nsteps >= 2) {
-        step_graph(nsteps / 2);
-        nsteps %= 2;
+    // steps replay the captured one-step graphs when nothing on the host has
+    // to happen between steps (no output units, no per-launch profiling)
+    if (graphs_ && !out_ && !profile_ && nsteps >= 1) {
+        step_graph(nsteps);
+        return;
     }
     step_launches(nsteps);
 }
 
-void Solver::step_graph(int npairs) {
+void Solver::step_graph(int nsteps) {
     if (graph_dirty_) {
         for (auto& g : graph_exec_)
             if (g) {
@@ -1048,11 +1048,14 @@ void Solver::step_graph(int npairs) {
         graph_dirty_ = false;
     }
     if (!step_dev_) cuda_check(cudaMalloc(&step_dev_, sizeof(int)), "cudaMalloc step counter");
-    // the graph bakes in which field buffer is read first: one graph per parity
-    cudaGraphExec_t& exec = graph_exec_[cur_];
-    if (!exec) {
-        // two steps: an even number of stages, so the field buffers end where they began
+    // a graph of one step bakes in which field buffer it reads first: one graph
+    // per parity; an odd number of stages leaves the other buffer current
+    const int flip = nstages_ & 1;
+    for (int par = 0; par < 2; par++) {
+        if (graph_exec_[par] || (par != cur_ && !flip)) continue;
+        if (par != cur_ && nsteps < 2) continue;   // captured when first needed
         const int cur0 = cur_, idx0 = step_index_;
+        cur_ = par;
         cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed), "begin capture");
         capturing_ = true;
         // if a stage throws while the stream captures, end the capture, drop the
@@ -1072,27 +1075,29 @@ void Solver::step_graph(int npairs) {
                 s.step_index_ = idx0;
             }
         } guard{*this, cur0, idx0};
-        for (int n = 0; n < 2; n++) {
-            for (int st = 0; st < nstages_; st++) {
-                if (precision_ == 0)
-                    stage_impl<double>(dt_, st, 0., true);
-                else
-                    stage_impl<float>(dt_, st, 0., true);
-            }
-            launch_step_advance(step_dev_, stream_);
+        for (int st = 0; st < nstages_; st++) {
+            if (precision_ == 0)
+                stage_impl<double>(dt_, st, 0., true);
+            else
+                stage_impl<float>(dt_, st, 0., true);
         }
+        launch_step_advance(step_dev_, stream_);
         guard.armed = false;
         capturing_ = false;
         cudaGraph_t g = nullptr;
         cuda_check(cudaStreamEndCapture(stream_, &g), "end capture");
-        cuda_check(cudaGraphInstantiate(&exec, g, 0), "graph instantiate");
+        const cudaError_t ie = cudaGraphInstantiate(&graph_exec_[par], g, 0);
         cudaGraphDestroy(g);
-        if (cur_ != cur0) throw std::runtime_error("graph capture left the field buffers swapped");
+        cur_ = cur0;
         step_index_ = idx0;
+        cuda_check(ie, "graph instantiate");
     }
     launch_set_step(step_dev_, step_index_, stream_);
-    for (int n = 0; n < npairs; n++) cuda_check(cudaGraphLaunch(exec, stream_), "graph launch");
-    step_index_ += 2 * npairs;
+    for (int n = 0; n < nsteps; n++) {
+        cuda_check(cudaGraphLaunch(graph_exec_[cur_], stream_), "graph launch");
+        cur_ ^= flip;
+    }
+    step_index_ += nsteps;
 }
 
 void Solver::step_launches(int nsteps) {
@@ -1467,6 +1472,14 @@ void Solver::get_fault(int iface, int which, double* out) {
     long long n = fault_count(iface, which);
     if (n <= 0) throw std::runtime_error("no such fault array");
     fetch_to(fault_array(ifaces_[iface], which), (size_t)n * sizeof(double), out);
+}
+
+void Solver::get_fault_async(int iface, int which, double* out) {
+    long long n = fault_count(iface, which);
+    if (n <= 0) throw std::runtime_error("no such fault array");
+    cuda_check(cudaMemcpyAsync(out, fault_array(ifaces_[iface], which), (size_t)n * sizeof(double),
+                               cudaMemcpyDeviceToHost, stream_),
+               "d2h");
 }
 
 void Solver::set_fault(int iface, int which, const double* in) {

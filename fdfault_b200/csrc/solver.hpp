@@ -53,6 +53,7 @@ class Solver {
     // volume component as the output list writes it at step tstep (absolute stress)
     void fetch_output_component(int comp, int tstep, double* out);
     void get_fault(int iface, int which, double* out);
+    void get_fault_async(int iface, int which, double* out);   // queued on the stream, no wait
     double* fault_ptr(int iface, int which) const;   // device array of a fault quantity (or null)
     void set_fault(int iface, int which, const double* in);
     long long fault_count(int iface, int which) const;
@@ -202,7 +203,7 @@ class Solver {
     int* step_dev_ = nullptr;
     cudaGraphExec_t graph_exec_[2] = {nullptr, nullptr};   // one per field-buffer parity
     void step_launches(int nsteps);
-    void step_graph(int npairs);
+    void step_graph(int nsteps);
     std::unique_ptr<OutputList> out_;
 
     // profiling

@@ -62,6 +62,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fdf_get_geometry.argtypes = [ctypes.c_void_p, c_int, c_int, dp]
     L.fdf_fault_count.argtypes = [ctypes.c_void_p, c_int, c_int, P(c_ll)]
     L.fdf_get_fault.argtypes = [ctypes.c_void_p, c_int, c_int, dp]
+    L.fdf_get_fault_async.argtypes = [ctypes.c_void_p, c_int, c_int, dp]
     L.fdf_set_fault.argtypes = [ctypes.c_void_p, c_int, c_int, dp]
     L.fdf_synchronize.argtypes = [ctypes.c_void_p]
     L.fdf_time_steps.argtypes = [ctypes.c_void_p, c_int, dp]
@@ -379,6 +380,17 @@ class Problem:
             raise ValueError("out must be a contiguous float64 array of %d values" % n)
         self._check(self._L.fdf_get_fault(self._h, iface, which, _dptr(out)))
         return out
+
+    def fault_async(self, iface: int, which: int, out: np.ndarray) -> None:
+        """Queue the copy of fault array `which` of interface `iface` into
+        `out` behind the work already queued and return at once; `out` holds the
+        values after the next synchronize() and must stay alive until then
+        (page-locked memory, e.g. a pinned torch tensor's numpy view, lets the
+        copy overlap host work)."""
+        n = self.fault_count(iface, which)
+        if out.dtype != np.float64 or out.size != n or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float64 array of %d values" % n)
+        self._check(self._L.fdf_get_fault_async(self._h, iface, which, _dptr(out)))
 
     def set_fault(self, iface: int, which: int, values: np.ndarray) -> None:
         a = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)

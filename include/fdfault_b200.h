@@ -118,6 +118,14 @@ int fdf_get_geometry(fdf_handle* h, int which, int comp, double* out);
 /* Number of values of a fault array of interface iface (0 if absent). */
 int fdf_fault_count(fdf_handle* h, int iface, int which, long long* n);
 int fdf_get_fault(fdf_handle* h, int iface, int which, double* out);
+/* Queues the same copy as fdf_get_fault behind the work already queued on the
+ * handle and returns without waiting: `out` holds the values once a later
+ * fdf_synchronize (or any call that waits) returns, and must stay valid until
+ * then; page-locked `out` lets the copy overlap host work.  For reading a
+ * step's fault output every step without stalling the next step's launch, in
+ * the way the reference's output units read the friction arrays after each
+ * step (src/outputunit.cpp:771-889). */
+int fdf_get_fault_async(fdf_handle* h, int iface, int which, double* out);
 int fdf_set_fault(fdf_handle* h, int iface, int which, const double* in);
 
 /* Waits for all queued device work; returns FDF_ERR_SOLVER if a kernel set
@@ -133,9 +141,10 @@ int fdf_time_steps(fdf_handle* h, int nsteps, double* ms);
 int fdf_profile(fdf_handle* h, int on);
 int fdf_profile_read(fdf_handle* h, int kernel, double* total_ms, long long* launches);
 
-/* fdf_step / fdf_solve / fdf_time_steps run whole pairs of steps by replaying
- * one captured CUDA graph of two steps when no output unit is due and
- * per-launch profiling is off (default on=1); results are identical to the
+/* fdf_step and fdf_time_steps run each step by replaying a captured CUDA
+ * graph of one step (one graph per field-buffer parity) when per-launch
+ * profiling is off (default on=1); fdf_solve, which writes output units
+ * between steps, launches stage by stage.  Results are identical to the
  * launch-by-launch path (the stage time comes from a device step counter). */
 int fdf_use_graphs(fdf_handle* h, int on);
 

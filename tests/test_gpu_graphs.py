@@ -1,8 +1,11 @@
-"""Stepping by CUDA-graph replay (pairs of steps, stage time from a device step
-counter) gives bit-identical fields, fault arrays and rupture times to
-launching every kernel from the host, for time-dependent loads (t0 > 0),
-slip-weakening time weakening, plasticity, STZ friction (plain and learned
-start) and the tiled FP32 kernel, with even and odd step counts."""
+"""Stepping by CUDA-graph replay (a one-step graph per field-buffer parity,
+stage time from a device step counter) gives bit-identical fields, fault
+arrays and rupture times to launching every kernel from the host, for
+time-dependent loads (t0 > 0), slip-weakening time weakening, plasticity, STZ
+friction (plain and learned start) and the FP32 marching kernel, with even and
+odd step counts and odd and even numbers of RK stages.  The fault read-back
+queued behind the steps (fdf_get_fault_async) returns the values the
+synchronous read returns."""
 
 import os
 
@@ -35,11 +38,12 @@ def run(infile, precision, graphs, chunks, setup=None):
 
 @pytest.mark.parametrize("name,precision", [("m2_perts", fs.FP64), ("m2_sw", fs.FP64), ("m2_plastic", fs.FP64),
                                             ("p3_sw", fs.FP32), ("p3_stz_files", fs.FP64),
-                                            ("p3_stz_files", fs.FP32)])
+                                            ("p3_stz_files", fs.FP32), ("m2_s3rk2", fs.FP64),
+                                            ("m2_rk1", fs.FP64), ("m2_s2rk4", fs.FP64)])
 def test_graph_replay_is_bit_identical(tmp_path, name, precision):
     prob = build_case(name, str(tmp_path))
     infile = prob.write(os.path.join(str(tmp_path), prob.name + ".in"))
-    chunks = [5, 2, 1, 4]   # odd and even counts: pairs replayed, the rest launched
+    chunks = [5, 2, 1, 4]   # odd and even counts, starting on either field buffer
     a, ia = run(infile, precision, False, chunks)
     b, ib = run(infile, precision, True, chunks)
     assert ia == ib == sum(chunks)
@@ -61,3 +65,18 @@ def test_graph_replay_learned_stz(tmp_path):
     b, _ = run(infile, fs.FP32, True, [12], setup)
     for k, (x, y) in enumerate(zip(a, b)):
         assert np.array_equal(x, y, equal_nan=True), k
+
+
+def test_async_fault_read_matches_sync(tmp_path):
+    prob = build_case("p3_sw", str(tmp_path))
+    infile = prob.write(os.path.join(str(tmp_path), prob.name + ".in"))
+    with fs.Problem(infile, precision=fs.FP32) as p:
+        outs = {w: np.full(p.fault_count(0, w), np.nan) for w in (fs.V, fs.U, fs.SX)}
+        for _ in range(3):
+            p.step(1)
+            for w, o in outs.items():
+                p.fault_async(0, w, o)
+        p.synchronize()
+        for w, o in outs.items():
+            assert np.array_equal(o, p.fault(0, w)), w
+
