@@ -4,8 +4,9 @@
 // 1541-2050), outer SAT (src/boundary.cpp:265-503) and RK update
 // (src/fields.cpp:293-309) as the tiled kernel in stage_fast.cu, with the
 // memory traffic organised so that no thread waits on a DRAM load of its own:
-//  * each CTA owns a TJ x TK tile of (j, k) columns of one block and marches
-//    along x through a chunk of planes; two CTAs share an SM;
+//  * each CTA owns an 8 x 32 tile of (j, k) columns of one block (12 x 16 over
+//    the last k columns when n2 mod 32 is small) and marches along x through
+//    a chunk of planes; two CTAs share an SM;
 //  * every plane's tile data arrives by TMA tensor copies into one of two
 //    shared-memory stages, issued by one thread a plane ahead and counted on
 //    an mbarrier: the centre plane i (fields, metric, Jacobian, rate register)
@@ -13,17 +14,20 @@
 //    the x fluxes J (m_x . sigma_c) and velocities enter the x window;
 //  * the x window of the interior stencil (planes i-H .. i+H of the thread's
 //    own column: three fluxes and three velocities each) lives in registers,
-//    so shared memory holds only the two stages and the y/z flux tiles;
+//    so shared memory holds only the two stages and the y/z flux tiles; a
+//    chunk fills its window by tensor copies through its second stage;
 //  * the y and z derivative inputs of the centre plane go to shared tiles
 //    with an (order-1) halo.  The centre boxes are staged 4 columns wider on
 //    each side, so the k halo comes from the stage; the j halo rows are loaded
 //    a plane ahead into registers by the threads that own them;
 //  * interior stencils are unrolled in the antisymmetric form with immediate
-//    coefficients; y closure rows (whole warps) use the tabulated rows and
-//    the two k-edge tiles use one tap row per lane, as in stage_fast.cu;
+//    coefficients; y closure rows use the tabulated rows and the k-edge
+//    tiles use one tap row per lane, as in stage_fast.cu;
 //  * the 2(order-1) planes at each x face, whose closure rows reach 3(order-1)
 //    planes, take their x derivatives from a pre-pass (k_xcl3d) that forms
 //    them from the stage-start fields in global memory;
+//  * plastic stages: the face-node kernel applies the return map to face
+//    nodes and k_return_map3 to the others on the last stage;
 //  * outer SATs: a pre-pass (k_ksat3d, one thread per k-face node) evaluates
 //    the SAT increments of the two k faces from the stage-start fields into a
 //    compact per-block buffer; the k-edge tiles stage their rows of it with
