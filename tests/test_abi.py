@@ -63,3 +63,5 @@ def test_null_handle_is_an_argument_error():
     L = solver.load_library()
     assert L.fdf_step(None, 1) == -1
     assert L.fdf_do_rk_stage(None, 0.1, 0, 0.0) == -1
+    assert L.fdf_set_plastic_rule(None, 1) == -1
+    assert L.fdf_get_fault_async(None, 0, 0, None) == -1
