@@ -38,6 +38,9 @@ PROFILE_WORKLOAD = dict(nx=201, ny=201, nz=201, h=0.1)
 CPU_SAMPLE = dict(nx=101, ny=51, nz=51, h=0.4)
 PROFILE_TRAFFIC = {1: os.path.join(HERE, "profiles", "volume_fast3d_planar3d.md"),
                    3: os.path.join(HERE, "profiles", "volume_regwindow3d_planar3d.md")}
+# steps of the end-to-end run (the workload itself runs 1500; the state upload
+# at its start is spread over these steps in h2d_bytes_per_step)
+E2E_STEPS = 300
 PLANAR_WORKLOAD_NAME = "planar3d: 2 blocks 401x201x201, slip weakening, log-normal mus, RK3 at CFL 0.2"
 KERNEL_NAMES = {0: "volume_exact", 1: "volume_tiled3d", 2: "volume_staged3d", 3: "volume_regwindow3d"}
 
@@ -375,7 +378,7 @@ def run_mode2(args, local):
         p.synchronize()
         clocks = ClockSampler(local)
         clocks.start()
-        ms = p.time_steps(args.steps)   # default path: pairs of steps replayed from a CUDA graph
+        ms = p.time_steps(args.steps)   # default path: each step replayed from a one-step CUDA graph
         clk = clocks.stop()
         p.profile(True)   # per-kernel event times: a separate pass, launched kernel by kernel
         p.step(min(args.steps, 20))
@@ -693,7 +696,7 @@ def main():
 
     precision = fs.FP32 if args.precision == "fp32" else fs.FP64
     tmp = tempfile.mkdtemp(prefix="fdf_bench_%d_" % rank)
-    nsteps_total = args.warmup + args.steps + max(args.e2e_steps, 100, 5 * args.steps) + 30
+    nsteps_total = args.warmup + args.steps + max(args.e2e_steps, E2E_STEPS, 5 * args.steps) + 30
     infile, prob = build_problem(tmp, nsteps_total, **(WORKLOAD if args.size == "full" else PROFILE_WORKLOAD))
     t_setup = time.perf_counter()
     p = fs.Problem(infile, precision=precision, device=local)
@@ -711,7 +714,7 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    ms = p.time_steps(args.steps)   # default path: pairs of steps replayed from a CUDA graph
+    ms = p.time_steps(args.steps)   # default path: each step replayed from a one-step CUDA graph
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -735,7 +738,7 @@ def main():
     # arrays that the reference's output units write every step (V, U, S, Sn,
     # Vx, Sx); the upload is counted in the timed region and spread over the
     # steps in h2d_bytes_per_step
-    ke = args.e2e_steps if args.e2e_steps > 0 else max(100, 5 * args.steps)
+    ke = args.e2e_steps if args.e2e_steps > 0 else max(E2E_STEPS, 5 * args.steps)
     fields = [torch.empty(nodes, dtype=torch.float64, pin_memory=True) for _ in range(p.nfields)]
     for c in range(p.nfields):
         fields[c].numpy()[:] = p.field(c)
