@@ -249,6 +249,21 @@ def c_p3_plastic_yield(tmp):
     return _yielding(_p3("p3_plastic_yield", tmp, nt=10), 0.5, True)
 
 
+def c_p3_hetmat_visits(tmp):
+    # a soft bottom plane (lambda + 2/3 G = 5.5): the reference's return-map
+    # loop, whose z index takes the bulk modulus (block.cpp:451-524), visits
+    # k = 0 and then k = trunc(5.5) + 1 = 6 of every column, where the usual
+    # moduli (53.4) send it past the block
+    p = _yielding(_p3("p3_hetmat_visits", tmp, nt=10), 0.5, True)
+    nx, ny, nz = p.nx
+    b = next(iter(p.blocks.values()))
+    rho, lam, g = (np.full((nx, ny, nz), v) for v in (b.rho, b.lam, b.g))
+    lam[:, :, 0] = 2.0
+    g[:, :, 0] = 5.25
+    p.matfile = P.write_material(os.path.join(tmp, "p3_hetmat_visits.mat"), rho, lam, g)
+    return p
+
+
 def c_p3_stz(tmp):
     p = _p3("p3_stz", tmp, nt=12)
     itf = p.interfaces[0]
@@ -330,6 +345,7 @@ CASES: Dict[str, Callable] = {
     "p3_xfault": c_p3_xfault, "p3_zfault": c_p3_zfault, "p3_stz_files": c_p3_stz_files,
     "p3_rough": c_p3_rough, "m2_hetmat": c_m2_hetmat, "m2_hetmat_plastic": c_m2_hetmat_plastic,
     "p3_hetmat": c_p3_hetmat, "m2_plastic_yield": c_m2_plastic_yield, "p3_plastic_yield": c_p3_plastic_yield,
+    "p3_hetmat_visits": c_p3_hetmat_visits,
 }
 
 # cases whose friction law calls exp/log inside the per-stage solve (STZ);

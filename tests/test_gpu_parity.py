@@ -65,7 +65,8 @@ def test_fp64_matches_reference(name, tmp_path):
 
 
 @pytest.mark.parametrize("name", ["m2_sw", "p3_sw", "m2_plastic", "p3_plastic", "m3", "m2_four_blocks", "m2_hetmat",
-                                  "p3_hetmat", "m2_hetmat_plastic", "m2_plastic_yield", "p3_plastic_yield"])
+                                  "p3_hetmat", "m2_hetmat_plastic", "m2_plastic_yield", "p3_plastic_yield",
+                                  "p3_hetmat_visits"])
 def test_fp64_stage_from_random_state(name, tmp_path):
     """One stage (A != 0) from a random state: fields, rates and fault arrays identical."""
     prob = cases.build_case(name, str(tmp_path), outputs=False)
