@@ -773,12 +773,13 @@ def main():
                 "algorithmic_bytes_per_node_stage": bps,
                 "traffic": (traffic_pn * nodes / nblocks) if traffic_pn else None}
     # per step: per stage the volume launches (tiled 3D: a marching and a face-node
-    # kernel per block; register window: k-face SAT and closure-plane pre-passes,
-    # marching kernel and x/y face-node kernel per block; staged: one per block;
-    # reference order: one for all blocks)
+    # kernel per block; register window: one pre-pass launch for all blocks (k-face
+    # SAT increments, closure-plane x derivatives), then a marching and an x/y
+    # face-node kernel per block; staged: one per block; reference order: one
+    # for all blocks)
     # and one interface launch per interface, plus the graph's step-counter kernel;
     # one counter reset per call
-    vol_per_stage = {0: 1, 1: 2 * nblocks, 2: nblocks, 3: 4 * nblocks}[vk]
+    vol_per_stage = {0: 1, 1: 2 * nblocks, 2: nblocks, 3: 2 * nblocks + 1}[vk]
     launches = args.steps * (nstages * (vol_per_stage + p.nifaces) + 1) + 1
     out = {"metric": METRIC, "value": value, "unit": "node-stage/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",

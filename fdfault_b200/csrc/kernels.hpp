@@ -86,6 +86,11 @@ void free_reg_maps(RegMapsHost* h);
 void launch_volume_reg3d(const VolumeArgs<float>& a, const BlockDev& b, int bi, const StageArgs& sa, int* status,
                          const RegMapsHost* maps, cudaStream_t s);
 bool reg3d_supported(const Layout& L, const BlockDev& b, int order);
+// the register-window kernel's pre-passes (k-face SAT increments, closure-plane
+// x derivatives) of blocks b0 .. b0+nb-1 (nb <= FDF_ALLB_MAX) in one launch,
+// before the blocks' marches; blks_dev is the device copy of the block table
+void launch_prepass_reg3d(const VolumeArgs<float>& a, const BlockDev* blks_dev, const BlockDev* blks, int b0,
+                          int nb, const StageArgs& sa, const RegMapsHost* maps, cudaStream_t s);
 // outer SATs and RK update of the face nodes of a 3D block, after a marching
 // kernel wrote their rate without the SAT (kdone: the k-face SATs are already
 // in the rate and nodes on k faces only are finished); plastic: the last

@@ -964,6 +964,15 @@ void Solver::stage_impl(double dt, int stage, double t, bool for_step) {
             cudaEventRecord(e0, stream_);
         }
         if constexpr (sizeof(T) == 4) {
+            // register window: the pre-passes of up to FDF_ALLB_MAX blocks in one
+            // launch, timed with the first of them
+            if (vk == 3 && P_.cdiss <= 0. && b % FDF_ALLB_MAX == 0) {
+                if (!reg_maps_)
+                    reg_maps_ = make_reg_maps(L_, (const float*)F_[0], (const float*)F_[1], (const float*)M_,
+                                              (const float*)J_, (const float*)DF_, blocks_.data(), (int)blocks_.size());
+                const int nb = std::min<int>(FDF_ALLB_MAX, (int)(blocks_.size() - b));
+                launch_prepass_reg3d(va, blocks_dev_, blocks_.data(), (int)b, nb, sa, reg_maps_, stream_);
+            }
             if (vk == 2) {
                 if (!staged_maps_)
                     staged_maps_ = make_staged_maps(L_, (const float*)F_[0], (const float*)F_[1], (const float*)M_,

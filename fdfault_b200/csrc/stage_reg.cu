@@ -24,11 +24,11 @@
 //    coefficients; y closure rows use the tabulated rows and the k-edge
 //    tiles use one tap row per lane, as in stage_fast.cu;
 //  * the 2(order-1) planes at each x face, whose closure rows reach 3(order-1)
-//    planes, take their x derivatives from a pre-pass (k_xcl3d) that forms
-//    them from the stage-start fields in global memory;
+//    planes, take their x derivatives from a pre-pass (k_prepass3d) that
+//    forms them from the stage-start fields in global memory;
 //  * plastic stages: the face-node kernel applies the return map to face
 //    nodes and k_return_map3 to the others on the last stage;
-//  * outer SATs: a pre-pass (k_ksat3d, one thread per k-face node) evaluates
+//  * outer SATs: the same pre-pass (one thread per k-face node) evaluates
 //    the SAT increments of the two k faces from the stage-start fields into a
 //    compact per-block buffer; the k-edge tiles stage their rows of it with
 //    the plane and finish k-face nodes themselves, so their stores stay whole
@@ -69,7 +69,7 @@ struct RegMapsHost {
     std::vector<float*> ksat;
     std::vector<int> jp;
     std::vector<CUtensorMap> kmap, ekmap;
-    // per block: x derivatives of the closure planes [slot][q][j][k] (see k_xcl3d)
+    // per block: x derivatives of the closure planes [slot][q][j][k] (see xcl_block)
     std::vector<float*> xcl;
     ~RegMapsHost() {
         for (float* p : ksat)
@@ -626,10 +626,11 @@ __global__ void __launch_bounds__(NTL, 2)
 // SAT increments of the two k faces of a block from the stage-start fields:
 // ks[side][c][i][jp] = the change the face's SAT makes to the rate of node
 // (i, j, k = 0 or n2-1).  One thread per face node, threads along j.
-__global__ void __launch_bounds__(128) k_ksat3d(VolumeArgs<float> a, BlockDev B, StageArgs sa, float* ks, int jp) {
-    const int side = blockIdx.z;
+// (bx, by, side): the 32 x 4 thread block's place in the (j, i, side) grid.
+__device__ __forceinline__ void ksat_block(const VolumeArgs<float>& a, const BlockDev& B, const StageArgs& sa,
+                                           float* ks, int jp, int bx, int by, int side) {
     if (!B.bactive[4 + side]) return;
-    const int j = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 4 + threadIdx.y;
+    const int j = bx * 32 + threadIdx.x, i = by * 4 + threadIdx.y;
     const int n0 = B.n[0], n1 = B.n[1];
     if (j >= n1 || i >= n0) return;
     const int k = side ? B.n[2] - 1 : 0;
@@ -652,12 +653,14 @@ __global__ void __launch_bounds__(128) k_ksat3d(VolumeArgs<float> a, BlockDev B,
 // xcl[slot][q][j][k], slot 0..NB-1 planes 0..NB-1, slot NB+m plane n0-NB+m,
 // q = 2c (flux) or 2c+1 (velocity).  One thread per (j, k) and face: each of
 // the 3(order-1) planes the closure rows reach is loaded once.
+// (bx, by, side): the 32 x 4 thread block's place in the (k, j, face) grid.
 template <int ORDER>
-__global__ void __launch_bounds__(128) k_xcl3d(VolumeArgs<float> a, BlockDev B, float* __restrict__ xcl) {
+__device__ __forceinline__ void xcl_block(const VolumeArgs<float>& a, const BlockDev& B, float* __restrict__ xcl,
+                                          int bx, int by, int side) {
     constexpr int H = ORDER - 1, NB = 2 * H, NTB = 3 * H;
     const int n0 = B.n[0], n1 = B.n[1], n2 = B.n[2];
-    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y;
-    const bool left = blockIdx.z == 0;
+    const int k = bx * 32 + threadIdx.x, j = by * 4 + threadIdx.y;
+    const bool left = side == 0;
     if (k >= n2 || j >= n1) return;
     const float sg = left ? 1.f : -1.f;
     const int cs = (int)a.L.cstride, s0 = (int)a.L.s0;
@@ -695,6 +698,36 @@ __global__ void __launch_bounds__(128) k_xcl3d(VolumeArgs<float> a, BlockDev B, 
             o[2 * c * pl] = d.x;
             o[(2 * c + 1) * pl] = d.y;
         }
+    }
+}
+
+// Both pre-passes of every block of a stage in one launch (each reads only the
+// stage-start fields): thread block t belongs to the block b with
+// start[b] <= t < start[b+1]; within it the first nk[b] evaluate the k-face
+// SAT increments (grid kx x ky x 2), the others the closure-plane x
+// derivatives (grid xx x xy x 2).  The block table is read from device memory.
+struct PrepTable {
+    int nblk;
+    int start[FDF_ALLB_MAX + 1];
+    int kx[FDF_ALLB_MAX], ky[FDF_ALLB_MAX], nk[FDF_ALLB_MAX], xx[FDF_ALLB_MAX], xy[FDF_ALLB_MAX],
+        jp[FDF_ALLB_MAX];
+    float* ks[FDF_ALLB_MAX];
+    float* xcl[FDF_ALLB_MAX];
+};
+
+template <int ORDER>
+__global__ void __launch_bounds__(128) k_prepass3d(VolumeArgs<float> a, const BlockDev* __restrict__ blks,
+                                                   StageArgs sa, const __grid_constant__ PrepTable P) {
+    int b = 0;
+    for (int q = 1; q < P.nblk; q++)
+        if ((int)blockIdx.x >= P.start[q]) b = q;
+    int t = blockIdx.x - P.start[b];
+    const BlockDev& B = blks[b];
+    if (t < P.nk[b]) {
+        ksat_block(a, B, sa, P.ks[b], P.jp[b], t % P.kx[b], (t / P.kx[b]) % P.ky[b], t / (P.kx[b] * P.ky[b]));
+    } else {
+        t -= P.nk[b];
+        xcl_block<ORDER>(a, B, P.xcl[b], t % P.xx[b], (t / P.xx[b]) % P.xy[b], t / (P.xx[b] * P.xy[b]));
     }
 }
 
@@ -746,10 +779,6 @@ void launch_order(const VolumeArgs<float>& a, const BlockDev& b, int bi, const S
     const int chunks = (b.n[0] + chunk - 1) / chunk;
     dim3 grid(tkm + edge, edge ? (tjm > tje ? tjm : tje) : tjm, chunks);
     const int fsel = (a.F == mh.F0) ? 0 : 1;
-    if (b.bactive[4] || b.bactive[5])
-        k_ksat3d<<<dim3((b.n[1] + 31) / 32, (b.n[0] + 3) / 4, 2), dim3(32, 4), 0, s>>>(a, b, sa, mh.ksat[bi],
-                                                                                      mh.jp[bi]);
-    k_xcl3d<ORDER><<<dim3((b.n[2] + 31) / 32, (b.n[1] + 3) / 4, 2), dim3(32, 4), 0, s>>>(a, b, mh.xcl[bi]);
     k_reg3d<ORDER><<<grid, NTL, SMEM, s>>>(a, b, sa, chunk, status, tkm, edge, mh.m, mh.me, fsel, mh.kmap[bi],
                                            mh.ekmap[bi], mh.xcl[bi]);
     // plasticity: face nodes get the return map in the face-node kernel, the
@@ -830,6 +859,33 @@ bool reg3d_supported(const Layout& L, const BlockDev& b, int order) {
     if (L.s1 % 4 != 0 || L.s0 % 4 != 0 || L.cstride % 4 != 0) return false;   // 16-byte row starts
     if (b.lo[2] % 4 != 0) return false;   // tiles start on 16-byte boundaries
     return true;
+}
+
+void launch_prepass_reg3d(const VolumeArgs<float>& a, const BlockDev* blks_dev, const BlockDev* blks, int b0,
+                          int nb, const StageArgs& sa, const RegMapsHost* maps, cudaStream_t s) {
+    if (nb > FDF_ALLB_MAX || nb < 1 || !maps) throw std::runtime_error("register-window pre-pass: bad block range");
+    PrepTable P{};
+    P.nblk = nb;
+    int t = 0;
+    for (int b = 0; b < nb; b++) {
+        const BlockDev& B = blks[b0 + b];
+        P.start[b] = t;
+        P.kx[b] = (B.n[1] + 31) / 32;
+        P.ky[b] = (B.n[0] + 3) / 4;
+        P.nk[b] = (B.bactive[4] || B.bactive[5]) ? P.kx[b] * P.ky[b] * 2 : 0;
+        P.xx[b] = (B.n[2] + 31) / 32;
+        P.xy[b] = (B.n[1] + 3) / 4;
+        P.jp[b] = maps->jp[b0 + b];
+        P.ks[b] = maps->ksat[b0 + b];
+        P.xcl[b] = maps->xcl[b0 + b];
+        t += P.nk[b] + P.xx[b] * P.xy[b] * 2;
+    }
+    P.start[nb] = t;
+    switch (a.order) {
+        case 2: k_prepass3d<2><<<t, dim3(32, 4), 0, s>>>(a, blks_dev + b0, sa, P); break;
+        case 3: k_prepass3d<3><<<t, dim3(32, 4), 0, s>>>(a, blks_dev + b0, sa, P); break;
+        default: k_prepass3d<4><<<t, dim3(32, 4), 0, s>>>(a, blks_dev + b0, sa, P); break;
+    }
 }
 
 void launch_volume_reg3d(const VolumeArgs<float>& a, const BlockDev& b, int bi, const StageArgs& sa, int* status,
