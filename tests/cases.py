@@ -314,6 +314,24 @@ def c_p3_zfault(tmp):
     return p
 
 
+def _with_material(p, name, tmp, seed):
+    p.name = name
+    P.layered_material(p, os.path.join(tmp, name + ".mat"), seed=seed)
+    return p
+
+
+def c_p3_hetmat_xfault(tmp):
+    return _with_material(c_p3_xfault(tmp), "p3_hetmat_xfault", tmp, 14)
+
+
+def c_p3_hetmat_stz(tmp):
+    return _with_material(c_p3_stz(tmp), "p3_hetmat_stz", tmp, 15)
+
+
+def c_m2_hetmat_locked(tmp):
+    return _with_material(c_m2_locked(tmp), "m2_hetmat_locked", tmp, 16)
+
+
 def c_m2_four_blocks(tmp):
     """Four blocks, four interfaces meeting at a corner node (shared finalisation)."""
     h = 0.1
@@ -345,12 +363,13 @@ CASES: Dict[str, Callable] = {
     "p3_xfault": c_p3_xfault, "p3_zfault": c_p3_zfault, "p3_stz_files": c_p3_stz_files,
     "p3_rough": c_p3_rough, "m2_hetmat": c_m2_hetmat, "m2_hetmat_plastic": c_m2_hetmat_plastic,
     "p3_hetmat": c_p3_hetmat, "m2_plastic_yield": c_m2_plastic_yield, "p3_plastic_yield": c_p3_plastic_yield,
-    "p3_hetmat_visits": c_p3_hetmat_visits,
+    "p3_hetmat_visits": c_p3_hetmat_visits, "p3_hetmat_xfault": c_p3_hetmat_xfault,
+    "p3_hetmat_stz": c_p3_hetmat_stz, "m2_hetmat_locked": c_m2_hetmat_locked,
 }
 
 # cases whose friction law calls exp/log inside the per-stage solve (STZ);
 # device and host libm differ in the last bit there
-LIBM_CASES = {"m2_stz", "p3_stz", "p3_stz_files"}
+LIBM_CASES = {"m2_stz", "p3_stz", "p3_stz_files", "p3_hetmat_stz"}
 
 
 def fault_fields(prob: P.Problem, iface: int = 0):
