@@ -56,3 +56,36 @@ def test_lognormal_field_statistics():
     assert abs(f.mean() - 0.677) < 0.01
     assert 0.02 < f.std() < 0.04
     assert (f > 0).all()
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_PY), reason="reference Python module not present")
+def test_material_file_matches_reference_module(tmp_path):
+    """A heterogeneous material file written by problems.write_material has the
+    bytes the reference's Python module writes for the same arrays
+    (python/fdfault/fields.py set_het_material / write_input)."""
+    import numpy as np
+    sys.path.insert(0, REF_PY)
+    try:
+        import warnings
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")
+            import fdfault
+    finally:
+        sys.path.remove(REF_PY)
+    os.chdir(tmp_path)
+    nx, ny = 21, 11
+    rng = np.random.default_rng(3)
+    mat = np.stack([base * (1. + 0.1 * rng.uniform(-1., 1., (nx, ny, 1))) for base in (P.RHO, P.LAM, P.G)])
+    r = fdfault.problem("matcmp")
+    r.set_ndim(2); r.set_mode(2)
+    r.set_nblocks((1, 1, 1)); r.set_nx_block(([nx], [ny], [1]))
+    r.set_block_lx((0, 0, 0), (2., 1.))
+    r.set_nt(1); r.set_cfl(0.3)
+    r.set_material(fdfault.material("elastic", P.RHO, P.LAM, P.G))
+    r.set_het_material(mat[..., 0])   # 2D: (3, nx, ny)
+    r.write_input()
+    mine = P.write_material(str(tmp_path / "mine.mat"), mat[0], mat[1], mat[2])
+    assert open(mine, "rb").read() == open(tmp_path / "matcmp.mat", "rb").read()
+    # the .in line names the file where the fields section expects it
+    assert str(tmp_path / "matcmp.mat") in open(tmp_path / "matcmp.in").read() or \
+        "matcmp.mat" in open(tmp_path / "matcmp.in").read()
