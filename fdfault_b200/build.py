@@ -27,7 +27,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 EXACT_CU = ["geometry.cu", "stage_exact.cu", "iface.cu", "noalloc.cu", "ensemble.cu", "energy.cu"]
-FAST_CU = ["stage_fast.cu", "stage_fast2d.cu", "stage_tma.cu", "stage_reg.cu", "mlp.cu"]
+FAST_CU = ["stage_fast.cu", "stage_fast2d.cu", "stage_tma.cu", "stage_reg.cu", "mlp.cu", "slab.cu"]
 HOST_CPP = ["input.cpp", "solver.cpp", "output.cpp", "api.cpp"]
 
 

@@ -179,6 +179,60 @@ int fdf_solve(fdf_handle* h) {
     return guarded(h, [&](fdf::Solver& s) { s.solve(); });
 }
 
+int fdf_step_stage(fdf_handle* h, int stage) {
+    return guarded(h, [&](fdf::Solver& s) { s.step_stage(stage); });
+}
+
+int fdf_set_x_range(fdf_handle* h, int x0, int x1) {
+    return guarded(h, [&](fdf::Solver& s) { s.set_x_range(x0, x1); });
+}
+
+int fdf_ghost_info(fdf_handle* h, int* planes, long long* count, int* elem_bytes) {
+    if (!planes || !count || !elem_bytes) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) {
+        *planes = s.ghost_planes();
+        *count = s.ghost_count();
+        *elem_bytes = s.precision() == 0 ? 8 : 4;
+    });
+}
+
+int fdf_pack_ghosts(fdf_handle* h, int side, void* dst) {
+    if (!dst) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { s.pack_ghosts(side, dst); });
+}
+
+int fdf_unpack_ghosts(fdf_handle* h, int side, const void* src) {
+    if (!src) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) { s.unpack_ghosts(side, src); });
+}
+
+int fdf_get_block(fdf_handle* h, int block, int* lo, int* n) {
+    if (!lo || !n) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) {
+        if (block < 0 || block >= (int)s.blocks().size()) throw std::runtime_error("block index out of range");
+        for (int d = 0; d < 3; d++) {
+            lo[d] = s.blocks()[block].lo[d];
+            n[d] = s.blocks()[block].n[d];
+        }
+    });
+}
+
+int fdf_get_interface(fdf_handle* h, int iface, int* direction, int* lo, int* n) {
+    if (!direction || !lo || !n) return FDF_ERR_ARG;
+    return guarded(h, [&](fdf::Solver& s) {
+        if (iface < 0 || iface >= (int)s.ifaces().size()) throw std::runtime_error("interface index out of range");
+        const fdf::IfaceDev& I = s.ifaces()[iface];
+        *direction = I.direction;
+        for (int d = 0; d < 3; d++) lo[d] = I.mlb[d];
+        n[0] = I.n0;
+        n[1] = I.n1;
+    });
+}
+
+int fdf_set_stream(fdf_handle* h, int own, void* stream) {
+    return guarded(h, [&](fdf::Solver& s) { s.set_stream(own != 0, static_cast<cudaStream_t>(stream)); });
+}
+
 int fdf_get_step(fdf_handle* h, int* step) {
     if (!step) return FDF_ERR_ARG;
     return guarded(h, [&](fdf::Solver& s) { *step = s.step_index(); });

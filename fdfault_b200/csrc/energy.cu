@@ -77,6 +77,7 @@ __global__ void __launch_bounds__(256) k_energy(EnergyArgs<T> a, BlockDev B, Nor
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         const int k = (int)(t % n2), j = (int)((t / n2) % n1), i = (int)(t / ((long long)n2 * n1));
+        if (i < B.xb || i >= B.xe) continue;   // plane summed by the process that updates it
         const long long id = (L.ndim == 3) ? node_index(L, B.lo[0] + i, B.lo[1] + j, B.lo[2] + k)
                                            : node_index(L, B.lo[0] + i, B.lo[1] + j, 0);
         double w = hw(W, i, n0) * hw(W, j, n1) * B.dx[0] * B.dx[1] * (double)a.J[id];
@@ -148,6 +149,7 @@ __global__ void __launch_bounds__(256) k_fault_power(Layout L, IfaceDev I, Block
         int g[3] = {I.mlb[0], I.mlb[1], I.mlb[2]};
         g[o0] += a;
         if (L.ndim == 3) g[o1] += b;
+        if (g[0] - B1.lo[0] < B1.xb || g[0] - B1.lo[0] >= B1.xe) continue;   // another process's plane
         const long long id = (L.ndim == 3) ? node_index(L, g[0], g[1], g[2]) : node_index(L, g[0], g[1], 0);
         double gn = 0.;
         for (int m = 0; m < L.ndim; m++) {

@@ -31,6 +31,10 @@ struct Layout {
 // per-block parameters used by the volume kernels
 struct BlockDev {
     int lo[3], n[3];      // first global node and node count per direction
+    // x planes this process updates, block-local [xb, xe): the whole block
+    // (0, n[0]) unless the domain is split into x slabs across processes;
+    // planes outside it are read (ghost planes) but not written
+    int xb, xe;
     double dx[3];         // computational grid spacing 1/(n-1) (block.cpp:772-774)
     double rho, lam, g;   // material
     double cp, cs, zp, zs, gamma;

@@ -551,6 +551,9 @@ __device__ __forceinline__ void interface_node(const IfaceArgs<T>& a, const Ifac
     const int o0 = (D == 0) ? 1 : 0, o1 = (D == 2) ? 1 : 2;
     pos[o0] += ii;
     pos[o1] += jj;
+    // fault nodes on x planes that another process updates are left to it
+    // (an x-normal fault goes with the minus side's last plane)
+    if (pos[0] - B1.lo[0] < B1.xb || pos[0] - B1.lo[0] >= B1.xe) return;
     const long long st[3] = {L.s0, L.s1, L.s2};
     const long long i1 = node_index(L, pos[0], pos[1], pos[2]);
     const long long i2 = i1 + st[D];

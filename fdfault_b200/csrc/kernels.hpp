@@ -138,6 +138,10 @@ template <typename T>
 void launch_store_component(const Layout& L, T* F, int comp, const double* in, cudaStream_t s);
 void launch_front(const IfaceDev& itf, double t, double value, cudaStream_t s);
 void launch_step_advance(int* step, cudaStream_t s);
+// x-slab ghost exchange: ncomp ranges of len elements at c * cstride + off of
+// the field buffer to (unpack 0) or from (unpack 1) a contiguous buffer
+void launch_ghost_copy(void* field, int elem_bytes, long long cstride, int ncomp, long long off, long long len,
+                       void* buf, int unpack, cudaStream_t s);
 void launch_set_step(int* step, int value, cudaStream_t s);
 
 }  // namespace fdf

@@ -141,6 +141,7 @@ Solver::Solver(const std::string& infile, int precision, int device) : precision
     // defer to the first fdf_get_field_noalloc call)
     noalloc_field_buffer(device);
     cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    own_stream_ = stream_;
     // RK coefficients: src/rk.cpp:8-98
     switch (P_.rkorder) {
         case 1:
@@ -252,6 +253,7 @@ Solver::Solver(const std::string& infile, int precision, int device) : precision
 
 Solver::~Solver() {
     if (stream_) cudaStreamSynchronize(stream_);
+    if (own_stream_ && own_stream_ != stream_) cudaStreamSynchronize(own_stream_);
     out_.reset();
     for (void* p : owned_) cudaFree(p);
     for (void* p : {F_[0], F_[1], DF_, FP_, M_, J_, (void*)M64_, (void*)J64_, (void*)X_, (void*)S_, (void*)ABS_,
@@ -273,7 +275,7 @@ Solver::~Solver() {
         cudaEventDestroy(pe.second.first);
         cudaEventDestroy(pe.second.second);
     }
-    if (stream_) cudaStreamDestroy(stream_);
+    if (own_stream_) cudaStreamDestroy(own_stream_);
 }
 
 // block geometry: block.cpp:183-246 (surfaces), 769-1046 (grid, metrics)
@@ -301,6 +303,8 @@ void Solver::setup_geometry() {
             g.n[d] = B.n[d];
             g.dx[d] = B.dx[d];
         }
+        B.xb = 0;
+        B.xe = B.n[0];
         for (int f = 0; f < 2 * ndim; f++) {
             int d = f / 2, o0, o1;
             other_dims(d, o0, o1);
@@ -941,6 +945,8 @@ void Solver::stage_impl(double dt, int stage, double t, bool for_step) {
     va.ABS = (sa.roundtrip && sa.last) ? ABS_ : nullptr;
     va.plastic_tensor = P_.plastic_tensor ? 1 : 0;
     const int vk = volume_kernel_active();
+    if (slab_ && vk != 0 && vk != 3)
+        throw std::runtime_error("x slabs run the register-window (3) or reference-order (0) volume kernel");
     // the reference-order kernel takes every block in one launch
     const bool all_exact = (sizeof(T) == 8 || vk == 0) && (int)blocks_.size() <= FDF_ALLB_MAX;
     if (all_exact) {
@@ -1036,7 +1042,96 @@ void Solver::do_rk_stage(double dt, int stage, double t) {
     cuda_check(cudaGetLastError(), "stage launch");
 }
 
+void Solver::step_stage(int stage) {
+    if (stage != stage_next_)
+        throw std::runtime_error("step_stage: expected stage " + std::to_string(stage_next_) + ", got " +
+                                 std::to_string(stage));
+    check_plastic_rule();
+    if (precision_ == 0)
+        stage_impl<double>(dt_, stage, (double)step_index_ * dt_, true);
+    else
+        stage_impl<float>(dt_, stage, (double)step_index_ * dt_, true);
+    cuda_check(cudaGetLastError(), "stage launch");
+    stage_next_ = (stage + 1) % nstages_;
+    if (stage_next_ == 0) step_index_++;
+}
+
+void Solver::set_x_range(int x0, int x1) {
+    const int nx = P_.nx[0];
+    if (x0 < 0 || x1 > nx || x0 >= x1) throw std::runtime_error("set_x_range: need 0 <= x0 < x1 <= nx");
+    const bool whole = (x0 == 0 && x1 == nx);
+    if (!whole) {
+        if (P_.ndim != 3) throw std::runtime_error("x slabs cover 3D problems");
+        if (P_.cdiss > 0.) throw std::runtime_error("x slabs: artificial dissipation is not supported");
+        const int vk = volume_kernel_active();
+        if (precision_ == 1 && vk != 0 && vk != 3)
+            throw std::runtime_error("x slabs run the register-window (3) or reference-order (0) volume kernel");
+        if (out_) throw std::runtime_error("x slabs: output units are written by whole-domain runs");
+        // a cut lies at least SLAB_MARGIN planes inside an x block: the closure
+        // rows and x faces (and any x-normal interface) stay with one slab, and
+        // a slab's first chunk starts past the closure rows
+        constexpr int SLAB_MARGIN = 16;
+        for (int c : {x0, x1}) {
+            if (c == 0 || c == nx) continue;
+            for (const auto& B : blocks_)
+                if (c >= B.lo[0] && c < B.lo[0] + B.n[0] &&
+                    (c - B.lo[0] < SLAB_MARGIN || B.lo[0] + B.n[0] - c < SLAB_MARGIN))
+                    throw std::runtime_error("set_x_range: cut at x = " + std::to_string(c) +
+                                             " is within 16 planes of an x block face");
+        }
+    }
+    synchronize();
+    for (auto& B : blocks_) {
+        B.xb = std::min(std::max(x0 - B.lo[0], 0), B.n[0]);
+        B.xe = std::min(std::max(x1 - B.lo[0], 0), B.n[0]);
+        if (B.xe < B.xb) B.xe = B.xb;
+    }
+    cuda_check(cudaMemcpyAsync(blocks_dev_, blocks_.data(), blocks_.size() * sizeof(BlockDev), cudaMemcpyHostToDevice,
+                               stream_),
+               "block table");
+    cuda_check(cudaStreamSynchronize(stream_), "block table");
+    slab_ = !whole;
+    xr0_ = x0;
+    xr1_ = x1;
+    graph_dirty_ = true;
+}
+
+long long Solver::ghost_count() const { return (long long)L_.nfields * ghost_planes() * L_.s0; }
+
+void Solver::pack_ghosts(int side, void* dst) {
+    if (!slab_) throw std::runtime_error("pack_ghosts: no x slab set");
+    if (side != 0 && side != 1) throw std::runtime_error("pack_ghosts: side is 0 or 1");
+    if (side == 0 ? xr0_ == 0 : xr1_ == P_.nx[0]) throw std::runtime_error("pack_ghosts: no neighbour on that side");
+    if (!dst) throw std::runtime_error("pack_ghosts: null buffer");
+    const int g = ghost_planes();
+    const long long off = (long long)(side == 0 ? xr0_ : xr1_ - g) * L_.s0;
+    launch_ghost_copy(F_[cur_], precision_ == 0 ? 8 : 4, L_.cstride, L_.nfields, off, (long long)g * L_.s0, dst, 0,
+                      stream_);
+    cuda_check(cudaGetLastError(), "ghost pack");
+}
+
+void Solver::unpack_ghosts(int side, const void* src) {
+    if (!slab_) throw std::runtime_error("unpack_ghosts: no x slab set");
+    if (side != 0 && side != 1) throw std::runtime_error("unpack_ghosts: side is 0 or 1");
+    if (side == 0 ? xr0_ == 0 : xr1_ == P_.nx[0]) throw std::runtime_error("unpack_ghosts: no neighbour on that side");
+    if (!src) throw std::runtime_error("unpack_ghosts: null buffer");
+    const int g = ghost_planes();
+    const long long off = (long long)(side == 0 ? xr0_ - g : xr1_) * L_.s0;
+    launch_ghost_copy(F_[cur_], precision_ == 0 ? 8 : 4, L_.cstride, L_.nfields, off, (long long)g * L_.s0,
+                      const_cast<void*>(src), 1, stream_);
+    cuda_check(cudaGetLastError(), "ghost unpack");
+}
+
+void Solver::set_stream(bool own, cudaStream_t s) {
+    if (capturing_) throw std::runtime_error("set_stream: a capture is in progress");
+    synchronize();
+    stream_ = own ? own_stream_ : s;
+}
+
 void Solver::step(int nsteps) {
+    if (slab_)
+        throw std::runtime_error("an x slab steps one stage at a time (step_stage) with a ghost exchange after each");
+    if (stage_next_ != 0) throw std::runtime_error("step: a step begun by step_stage is unfinished");
     check_plastic_rule();
     // steps replay the captured one-step graphs when nothing on the host has
     // to happen between steps (no output units, no per-launch profiling)
@@ -1136,6 +1231,7 @@ void Solver::fetch_output_component(int comp, int tstep, double* out) {
 }
 
 void Solver::solve() {
+    if (slab_) throw std::runtime_error("solve runs the whole domain: set_x_range(0, nx) first");
     if (!out_) {
         out_.reset(new OutputList(*this));
         if (out_->needs_abs_stress() && !ABS_) {
@@ -1176,6 +1272,22 @@ void Solver::energy(bool with_rate, double out[8]) {
         }
         B_[0] = b0;
         cuda_check(cudaGetLastError(), "energy rate stage");
+        if (slab_) {
+            // the stage wrote only this slab's planes into the other buffer:
+            // carry the ghost planes over from the one it read
+            const size_t es = precision_ == 0 ? 8 : 4;
+            const long long g = ghost_planes();
+            for (int side = 0; side < 2; side++) {
+                if (side == 0 ? xr0_ == 0 : xr1_ == P_.nx[0]) continue;
+                const long long off = (side == 0 ? xr0_ - g : (long long)xr1_) * L_.s0;
+                for (int c = 0; c < L_.nfields; c++) {
+                    const size_t at = (size_t)(c * L_.cstride + off) * es;
+                    cuda_check(cudaMemcpyAsync((char*)F_[cur_] + at, (const char*)F_[1 - cur_] + at,
+                                               (size_t)(g * L_.s0) * es, cudaMemcpyDeviceToDevice, stream_),
+                               "ghost planes");
+                }
+            }
+        }
     }
     if (!energy_dev_) cuda_check(cudaMalloc(&energy_dev_, 8 * sizeof(double)), "cudaMalloc energy accumulators");
     cuda_check(cudaMemsetAsync(energy_dev_, 0, 8 * sizeof(double), stream_), "memset");

@@ -37,6 +37,28 @@ class Solver {
     void step(int nsteps);
     // the whole problem::solve loop including output units and fronts
     void solve();
+    // stage `stage` of the current step exactly as step() runs it; the last
+    // stage advances the step counter (stages must come in order)
+    void step_stage(int stage);
+
+    // x slabs (fields.cpp:276-291, cartesian.cpp:88-165 split the domain the
+    // same way across MPI ranks): this process updates the global x planes
+    // [x0, x1) and reads order-1 ghost planes on each side, which the caller
+    // refreshes after every stage from the neighbouring slabs (pack_ghosts /
+    // unpack_ghosts).  (0, nx) is the whole domain.
+    void set_x_range(int x0, int x1);
+    bool slab() const { return slab_; }
+    int ghost_planes() const { return P_.sbporder - 1; }
+    long long ghost_count() const;   // elements of one side's ghost exchange
+    // side 0: the first ghost_planes() updated planes (the lower neighbour's
+    // upper ghosts); side 1: the last ones.  dst/src are device buffers of
+    // ghost_count() elements in the fields' precision.
+    void pack_ghosts(int side, void* dst);
+    // side 0: the ghost planes below x0; side 1: those from x1 on
+    void unpack_ghosts(int side, const void* src);
+    // run on the caller's stream (own = false) or the handle's own (own = true)
+    void set_stream(bool own, cudaStream_t s);
+
     // reset the step counter (tests that drive stages directly)
     void set_step_index(int i) { step_index_ = i; }
     int step_index() const { return step_index_; }
@@ -149,6 +171,10 @@ class Solver {
     int precision_ = 0;   // 0 exact FP64, 1 FP32 fields
     int device_ = 0;
     cudaStream_t stream_ = nullptr;
+    cudaStream_t own_stream_ = nullptr;   // created by the handle; stream_ may be the caller's
+    bool slab_ = false;                   // x range narrower than the domain
+    int xr0_ = 0, xr1_ = 0;               // updated global x planes [xr0_, xr1_)
+    int stage_next_ = 0;                  // next stage of step_stage
     double dt_ = 0, ttot_ = 0, cfl_ = 0;
     int nt_ = 0, nstages_ = 0;
     double A_[5] = {0}, B_[5] = {0}, C_[6] = {0};

@@ -51,7 +51,8 @@ __global__ void __launch_bounds__(128) k_volume_exact_all(VolumeArgs<T> a, const
 
 template <typename T>
 void launch_volume_exact(const VolumeArgs<T>& a, const BlockDev& b, const StageArgs& sa, cudaStream_t s) {
-    long long nn = (long long)b.n[0] * b.n[1] * b.n[2];
+    long long nn = (long long)(b.xe - b.xb) * b.n[1] * b.n[2];
+    if (nn <= 0) return;
     unsigned grid = (unsigned)((nn + 127) / 128);
     // heterogeneous material: modes II and 3D (mode III is rejected at input)
     if (a.L.ndim == 3) {
@@ -76,9 +77,10 @@ void launch_volume_exact_all(const VolumeArgs<T>& a, const BlockDev* blks_dev, c
     long long n = 0;
     for (int b = 0; b < FDF_ALLB_MAX; b++) {
         r.start[b] = n;
-        if (b < nb) n += (long long)blks[b].n[0] * blks[b].n[1] * blks[b].n[2];
+        if (b < nb) n += (long long)(blks[b].xe - blks[b].xb) * blks[b].n[1] * blks[b].n[2];
     }
     r.start[FDF_ALLB_MAX] = n;   // ranges of absent blocks are empty and never selected
+    if (n <= 0) return;
     const unsigned grid = (unsigned)((n + 127) / 128);
     const bool het = nb > 0 && blks[0].mat != nullptr;   // one material array for all blocks
     if (a.L.ndim == 3) {

@@ -22,12 +22,13 @@ template <typename T, int NDIM, int MODE, bool HET = false>
 __device__ __forceinline__ void volume_node(const VolumeArgs<T>& a, const BlockDev& B, const StageArgs& sa,
                                             long long t) {
     const Layout& L = a.L;
-    const long long nn = (long long)B.n[0] * B.n[1] * B.n[2];
+    // t counts the nodes of the planes this process updates (xb <= p[0] < xe)
+    const long long nn = (long long)(B.xe - B.xb) * B.n[1] * B.n[2];
     if (t >= nn) return;
     int p[3];
     p[2] = (int)(t % B.n[2]);
     p[1] = (int)((t / B.n[2]) % B.n[1]);
-    p[0] = (int)(t / ((long long)B.n[2] * B.n[1]));
+    p[0] = B.xb + (int)(t / ((long long)B.n[2] * B.n[1]));
     const long long id = node_index(L, B.lo[0] + p[0], B.lo[1] + p[1], B.lo[2] + p[2]);
     const long long cs = L.cstride;
     const int order = a.order;

@@ -464,6 +464,7 @@ __global__ void __launch_bounds__(128) k_faces3d(VolumeArgs<float> a, BlockDev B
         j = ub;
         k = at;
     }
+    if (i < B.xb || i >= B.xe) return;                // plane updated by another process
     if (d >= 1 && (i == 0 || i == n0 - 1)) return;   // belongs to an x face
     if (d == 2 && (j == 0 || j == n1 - 1)) return;   // belongs to a y face
     const Layout& L = a.L;
@@ -507,10 +508,12 @@ __global__ void __launch_bounds__(128) k_faces3d(VolumeArgs<float> a, BlockDev B
 // would exceed.
 __global__ void __launch_bounds__(256) k_return_map3(VolumeArgs<float> a, BlockDev B, StageArgs sa, int kall) {
     const int n1i = B.n[1] - 2, n2i = kall ? B.n[2] : B.n[2] - 2;
+    // interior planes this process updates: max(1, xb) <= i < min(n0 - 1, xe)
+    const int i0 = max(1, B.xb), i1 = min(B.n[0] - 1, B.xe);
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= (long long)(B.n[0] - 2) * n1i * n2i) return;
+    if (t >= (long long)(i1 - i0) * n1i * n2i) return;
     const int k = (kall ? 0 : 1) + (int)(t % n2i), j = 1 + (int)((t / n2i) % n1i),
-              i = 1 + (int)(t / ((long long)n2i * n1i));
+              i = i0 + (int)(t / ((long long)n2i * n1i));
     if ((k == 0 && B.defer[4]) || (k == B.n[2] - 1 && B.defer[5])) return;
     const Layout& L = a.L;
     const long long cs = L.cstride;
@@ -584,7 +587,9 @@ void launch_faces3d(const VolumeArgs<float>& a, const BlockDev& b, const StageAr
 
 void launch_return_map3(const VolumeArgs<float>& a, const BlockDev& b, const StageArgs& sa, bool kall,
                         cudaStream_t s) {
-    const long long nin = (long long)(b.n[0] - 2) * (b.n[1] - 2) * (kall ? b.n[2] : b.n[2] - 2);
+    const int i0 = b.xb > 1 ? b.xb : 1, i1 = b.xe < b.n[0] - 1 ? b.xe : b.n[0] - 1;
+    const long long nin = (long long)(i1 - i0) * (b.n[1] - 2) * (kall ? b.n[2] : b.n[2] - 2);
+    if (nin <= 0) return;
     k_return_map3<<<(unsigned)((nin + 255) / 256), 256, 0, s>>>(a, b, sa, kall ? 1 : 0);
 }
 

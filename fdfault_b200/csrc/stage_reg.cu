@@ -180,8 +180,10 @@ __device__ __forceinline__ void reg_march(const VolumeArgs<float>& a, const Bloc
     const bool ownk = (k >= n2) ? false : (k >= n2 - NB) ? lastk : (k >= T.kown0 && k < T.kown1);
     const bool ownj = (j >= n1 - NB) ? lastj : (j / TJ == T.by);
     const bool owner = ownk && ownj;
-    const int ib = blockIdx.z * chunk;
-    const int ie = min(n0, ib + chunk);
+    // chunks tile the planes this process updates, [xb, xe); the x window and
+    // the closure tests stay in block coordinates
+    const int ib = B.xb + blockIdx.z * chunk;
+    const int ie = min(B.xe, ib + chunk);
     if (ib >= ie) return;
     const long long wlim = sa.wait_limit != 0 ? sa.wait_limit : (1LL << 22);
 
@@ -631,8 +633,9 @@ __device__ __forceinline__ void ksat_block(const VolumeArgs<float>& a, const Blo
                                            float* ks, int jp, int bx, int by, int side) {
     if (!B.bactive[4 + side]) return;
     const int j = bx * 32 + threadIdx.x, i = by * 4 + threadIdx.y;
-    const int n0 = B.n[0], n1 = B.n[1];
-    if (j >= n1 || i >= n0) return;
+    const int n1 = B.n[1];
+    if (j >= n1 || i < B.xb || i >= B.xe) return;   // planes this process updates
+    const int n0 = B.n[0];
     const int k = side ? B.n[2] - 1 : 0;
     const long long cs = a.L.cstride;
     const long long id = node_index(a.L, B.lo[0] + i, B.lo[1] + j, B.lo[2] + k);
@@ -662,6 +665,7 @@ __device__ __forceinline__ void xcl_block(const VolumeArgs<float>& a, const Bloc
     const int k = bx * 32 + threadIdx.x, j = by * 4 + threadIdx.y;
     const bool left = side == 0;
     if (k >= n2 || j >= n1) return;
+    if (B.xe <= B.xb || (left ? B.xb >= NB : B.xe <= n0 - NB)) return;   // no closure plane of this face updated here
     const float sg = left ? 1.f : -1.f;
     const int cs = (int)a.L.cstride, s0 = (int)a.L.s0;
     const int colbase = B.lo[0] * s0 + (B.lo[1] + j) * (int)a.L.s1 + (B.lo[2] + k);
@@ -775,8 +779,10 @@ void launch_order(const VolumeArgs<float>& a, const BlockDev& b, int bi, const S
     const int tkm = edge ? b.n[2] / TKM : (b.n[2] + TKM - 1) / TKM;
     const int tjm = (b.n[1] + TJM - 1) / TJM, tje = (b.n[1] + TJE - 1) / TJE;
     const int tiles = tkm * tjm + (edge ? tje : 0);
-    const int chunk = pick_chunk(b.n[0], tiles, occ[dev & 31] * nsm, ORDER - 1);
-    const int chunks = (b.n[0] + chunk - 1) / chunk;
+    const int nown = b.xe - b.xb;   // planes this process updates
+    if (nown <= 0) return;
+    const int chunk = pick_chunk(nown, tiles, occ[dev & 31] * nsm, ORDER - 1);
+    const int chunks = (nown + chunk - 1) / chunk;
     dim3 grid(tkm + edge, edge ? (tjm > tje ? tjm : tje) : tjm, chunks);
     const int fsel = (a.F == mh.F0) ? 0 : 1;
     k_reg3d<ORDER><<<grid, NTL, SMEM, s>>>(a, b, sa, chunk, status, tkm, edge, mh.m, mh.me, fsel, mh.kmap[bi],

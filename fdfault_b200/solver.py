@@ -103,6 +103,14 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.fdf_ensemble_check_status.argtypes = [vp]
     L.fdf_ensemble_last_error.argtypes = [vp]
     L.fdf_ensemble_last_error.restype = ctypes.c_char_p
+    L.fdf_step_stage.argtypes = [ctypes.c_void_p, c_int]
+    L.fdf_set_x_range.argtypes = [ctypes.c_void_p, c_int, c_int]
+    L.fdf_ghost_info.argtypes = [ctypes.c_void_p, P(c_int), P(c_ll), P(c_int)]
+    L.fdf_pack_ghosts.argtypes = [ctypes.c_void_p, c_int, vp]
+    L.fdf_unpack_ghosts.argtypes = [ctypes.c_void_p, c_int, vp]
+    L.fdf_get_block.argtypes = [ctypes.c_void_p, c_int, P(c_int), P(c_int)]
+    L.fdf_set_stream.argtypes = [ctypes.c_void_p, c_int, vp]
+    L.fdf_get_interface.argtypes = [ctypes.c_void_p, c_int, P(c_int), P(c_int), P(c_int)]
     L.fdf_last_error.argtypes = [ctypes.c_void_p]
     L.fdf_last_error.restype = ctypes.c_char_p
     _lib = L
@@ -180,6 +188,58 @@ class Problem:
 
     def solve(self) -> None:
         self._check(self._L.fdf_solve(self._h))
+
+    def step_stage(self, stage: int) -> None:
+        """Stage `stage` of the current step as step() runs it; the last stage
+        advances the step counter."""
+        self._check(self._L.fdf_step_stage(self._h, stage))
+
+    # --- x slabs (one process per GPU; fdfault_b200.slabs drives them) ----
+    def set_x_range(self, x0: int, x1: int) -> None:
+        """Update only the global x planes [x0, x1) (cartesian.cpp:88-165 splits
+        the reference's domain across MPI ranks)."""
+        self._check(self._L.fdf_set_x_range(self._h, x0, x1))
+
+    def ghost_info(self) -> Tuple[int, int, int]:
+        """(ghost planes per side, elements of one side's exchange, bytes per element)."""
+        g, n, e = ctypes.c_int(), ctypes.c_longlong(), ctypes.c_int()
+        self._check(self._L.fdf_ghost_info(self._h, ctypes.byref(g), ctypes.byref(n), ctypes.byref(e)))
+        return g.value, n.value, e.value
+
+    def pack_ghosts(self, side: int, dst_ptr: int) -> None:
+        """Side 0: the slab's first planes; side 1: its last ones, into the device buffer at dst_ptr."""
+        self._check(self._L.fdf_pack_ghosts(self._h, side, ctypes.c_void_p(dst_ptr)))
+
+    def unpack_ghosts(self, side: int, src_ptr: int) -> None:
+        """Side 0: the ghost planes below the slab; side 1: those above it, from the device buffer."""
+        self._check(self._L.fdf_unpack_ghosts(self._h, side, ctypes.c_void_p(src_ptr)))
+
+    def block(self, b: int) -> Tuple[Tuple[int, int, int], Tuple[int, int, int]]:
+        """(first global node, node counts) of block b."""
+        lo, n = (ctypes.c_int * 3)(), (ctypes.c_int * 3)()
+        self._check(self._L.fdf_get_block(self._h, b, lo, n))
+        return tuple(lo), tuple(n)
+
+    def interface(self, iface: int) -> Tuple[int, Tuple[int, int, int], Tuple[int, int]]:
+        """(normal direction, first global node of the minus-side face, face node counts)."""
+        d, lo, n = ctypes.c_int(), (ctypes.c_int * 3)(), (ctypes.c_int * 2)()
+        self._check(self._L.fdf_get_interface(self._h, iface, ctypes.byref(d), lo, n))
+        return d.value, tuple(lo), tuple(n)
+
+    @property
+    def torch_device(self):
+        """The torch device that holds this problem's buffers."""
+        import torch
+
+        return torch.device("cuda", self.device)
+
+    def set_stream(self, stream: Optional[int]) -> None:
+        """Launch on the CUDA stream handle `stream` (an int, 0 the legacy
+        default stream), or on the problem's own stream when None."""
+        if stream is None:
+            self._check(self._L.fdf_set_stream(self._h, 1, None))
+        else:
+            self._check(self._L.fdf_set_stream(self._h, 0, ctypes.c_void_p(stream)))
 
     @property
     def step_index(self) -> int:

@@ -81,6 +81,44 @@ int fdf_step(fdf_handle* h, int nsteps);
  * steps, writes the output units and the rupture fronts. */
 int fdf_solve(fdf_handle* h);
 
+/* Stage `stage` of the current step as fdf_step runs it (the loop body of
+ * src/problem.cpp:151-168 split at its domain::do_rk_stage calls); the last
+ * stage advances the step counter.  Stages come in order 0, 1, ...; an x
+ * slab exchanges its ghost planes between two calls. */
+int fdf_step_stage(fdf_handle* h, int stage);
+
+/* Multi-GPU x slabs.  The reference splits its domain across MPI ranks
+ * (src/cartesian.cpp:88-165) and swaps ghost planes after every stage
+ * (fields::exchange_neighbors, src/fields.cpp:276-291, called from
+ * src/domain.cpp:228-305).  Here each process updates the global x planes
+ * [x0, x1) of its own copy of the grid (3D; volume kernel 0 or 3; no
+ * dissipation; each cut at least 16 planes inside an x block) and steps with
+ * fdf_step_stage; after each stage it packs its edge planes for its
+ * neighbours and unpacks theirs into its ghost planes.  (0, nx) is the whole
+ * domain again.  fdf_step and fdf_solve refuse a slab. */
+int fdf_set_x_range(fdf_handle* h, int x0, int x1);
+/* planes: ghost planes per side (sbporder - 1); count: elements of one side's
+ * exchange buffer; elem_bytes: 8 (FP64 problem) or 4 (FP32). */
+int fdf_ghost_info(fdf_handle* h, int* planes, long long* count, int* elem_bytes);
+/* side 0: the slab's first `planes` planes into dst (for the lower
+ * neighbour); side 1: its last ones (for the upper neighbour).  dst and src
+ * are device buffers of `count` elements, ordered on the handle's stream. */
+int fdf_pack_ghosts(fdf_handle* h, int side, void* dst);
+/* side 0: src into the ghost planes below x0; side 1: into those from x1. */
+int fdf_unpack_ghosts(fdf_handle* h, int side, const void* src);
+/* First global node lo[3] and node counts n[3] of block `block` (blocks in
+ * the order of the input file's block list). */
+int fdf_get_block(fdf_handle* h, int block, int* lo, int* n);
+/* Interface `iface`: its normal direction (0 x, 1 y, 2 z), the minus-side
+ * face's first global node lo[3] and the face's node counts n[2]; fault node
+ * (a, b) lies at lo + a along the first other direction and + b along the
+ * second (x before y before z). */
+int fdf_get_interface(fdf_handle* h, int iface, int* direction, int* lo, int* n);
+/* Launch on the caller's CUDA stream (own = 0; e.g. the stream a collective
+ * library waits on) or the handle's own stream again (own = 1).  Waits for
+ * the work already queued first. */
+int fdf_set_stream(fdf_handle* h, int own, void* stream);
+
 /* Index of the next step to run. */
 int fdf_get_step(fdf_handle* h, int* step);
 int fdf_set_step(fdf_handle* h, int step);
