@@ -64,6 +64,10 @@ def parse():
                          "rupture in FP64; ensemble: 256 2D ruptures of uneven sizes, batched; rough: "
                          "rough fault with plasticity, two blocks of 601x301x301, FP32")
     ap.add_argument("--members", type=int, default=256, help="ensemble members (all ranks together)")
+    ap.add_argument("--decomp", default="replicas", choices=["replicas", "slabs"],
+                    help="planar workload on N GPUs: replicas (each rank its own copy, weak scaling) or "
+                         "slabs (one problem split along x, ghost planes exchanged over NCCL after every "
+                         "stage, strong scaling)")
     ap.add_argument("--volume-kernel", type=int, default=3, choices=[0, 1, 2, 3],
                     help="FP32 3D volume kernel: 0 reference order, 1 tiled, 2 staged (TMA), "
                          "3 register window (TMA-staged planes, default)")
@@ -672,9 +676,119 @@ def run_extras():
     return res
 
 
+def run_slabs(args, rank, world, local):
+    """The planar workload split into ``world`` x slabs, one per GPU (strong
+    scaling): every rank steps stage by stage on one CUDA stream and swaps its
+    edge planes with its neighbours over NCCL after each stage
+    (fdfault_b200.slabs).  value = the whole grid's node-stages / the slowest
+    rank's device time."""
+    import datetime
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.barrier()   # communicator set up before the first point-to-point exchange
+    from fdfault_b200 import replicas, slabs
+    from fdfault_b200 import solver as fs
+
+    precision = fs.FP32 if args.precision == "fp32" else fs.FP64
+    tmp = tempfile.mkdtemp(prefix="fdf_slab_%d_" % rank)
+    ke = args.e2e_steps if args.e2e_steps > 0 else max(E2E_STEPS, 5 * args.steps)
+    infile, _ = build_problem(tmp, args.warmup + args.steps + ke + 30,
+                              **(WORKLOAD if args.size == "full" else PROFILE_WORKLOAD))
+    p = fs.Problem(infile, precision=precision, device=local)
+    vk = p.set_volume_kernel(args.volume_kernel)
+    nodes, nstages, nblocks = p.nxyz, p.nstages, int(np.prod(p.nblocks))
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        run = slabs.SlabRun(p, rank, world, transport=slabs.DistTransport(rank, world) if world > 1 else None)
+        owned = (run.x1 - run.x0) * (nodes // p.nx[0])
+        run.step(args.warmup)
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local)
+        clocks.start()
+        time.sleep(0.3)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run.step(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        ms = e0.elapsed_time(e1)
+        clk = clocks.stop()
+        # per-kernel event times of this rank's volume stage
+        p.profile(True)
+        run.step(min(args.steps, 20))
+        vol_ms, vol_n = p.profile_read(0)
+        p.profile(False)
+        p.synchronize()
+        # end to end: state upload from pinned host memory, then steps with this
+        # rank's on-fault arrays read back into pinned buffers after every step
+        fields = [torch.empty(nodes, dtype=torch.float64, pin_memory=True) for _ in range(p.nfields)]
+        for c in range(p.nfields):
+            fields[c].numpy()[:] = p.field(c)
+        outs = [torch.empty(p.fault_count(0, w), dtype=torch.float64, pin_memory=True)
+                for w in (fs.V, fs.U, fs.S, fs.SN, fs.VX, fs.SX)]
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for c in range(p.nfields):
+            p.set_field(c, fields[c].numpy())
+        for _ in range(ke):
+            run.step(1)
+            for w, o in zip((fs.V, fs.U, fs.S, fs.SN, fs.VX, fs.SX), outs):
+                p.fault_async(0, w, o.numpy())
+        p.synchronize()
+        te = time.perf_counter() - t0
+    work, ms = replicas.reduce_totals(float(owned * nstages * args.steps), ms, device="cuda")
+    e2e_work, te = replicas.reduce_totals(float(owned * nstages * ke), te, device="cuda")
+    bps = p.bytes_per_node_stage()
+    peak, peak_kind = measured_peak()
+    vol_avg_ms = vol_ms / max(vol_n, 1)
+    achieved = bps * owned / nblocks / (vol_avg_ms * 1e-3) / 1e9
+    vol_per_stage = {0: 1, 1: 2 * nblocks, 2: nblocks, 3: 2 * nblocks + 1}[vk]
+    launches = args.steps * nstages * (vol_per_stage + p.nifaces + 2 * len(run.sides))
+    out = {"metric": METRIC, "value": work / (ms * 1e-3), "unit": "node-stage/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+           "scaling": "strong", "vs_baseline": None, "dtype": "f32" if precision == fs.FP32 else "f64",
+           "data": "synthetic",
+           "config": {"workload": PLANAR_WORKLOAD_NAME if args.size == "full" else "planar3d profile size",
+                      "nodes": nodes, "stages_per_step": nstages, "parallelism": "x slabs %s" % run.slabs,
+                      "ghost_bytes_per_stage_rank0": run.ghost_bytes_per_exchange,
+                      "l2": "inputs larger than L2"},
+           "clocks": clk,
+           "e2e": {"value": e2e_work / te, "unit": "node-stage/s",
+                   "h2d_bytes_per_step": 8 * nodes * p.nfields / ke,
+                   "d2h_bytes_per_step": sum(o.numel() * 8 for o in outs), "steps": ke},
+           "gpu_launches": launches,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "peak_source": peak_kind, "kernel": KERNEL_NAMES[vk],
+                        "algorithmic_bytes_per_node_stage": bps, "traffic": None}}
+    run.release()
+    p.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.impl == "b200" and args.config == "planar" and args.decomp == "slabs":
+        run_slabs(args, rank, world, local)
+        return
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
         return

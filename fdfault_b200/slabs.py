@@ -251,28 +251,50 @@ class LocalSlabs:
     whole-domain run on one GPU.  The slabs run one after another (no kernel
     waits on another slab's kernel)."""
 
-    def __init__(self, problems: Sequence, slabs: Optional[Sequence[Tuple[int, int]]] = None):
+    def __init__(self, problems: Sequence, slabs: Optional[Sequence[Tuple[int, int]]] = None, stream=None):
+        """``stream``: a ``torch.cuda.Stream`` on which every slab launches
+        (``Problem.set_stream``, as a rank of a multi-GPU run launches on the
+        stream its NCCL transfers are ordered against), with the copies queued
+        on it too; None keeps each slab on its own stream and synchronises
+        around the copies."""
         import torch
 
         self.problems = list(problems)
         world = len(self.problems)
         self.slabs = list(slabs) if slabs is not None else plan_slabs(x_blocks(self.problems[0]), world)
+        self.stream = stream
         self.runs = []
         for r, p in enumerate(self.problems):
-            self.runs.append(SlabRun(p, r, world, transport=None, slabs=self.slabs, use_current_stream=False))
+            if stream is None:
+                self.runs.append(SlabRun(p, r, world, transport=None, slabs=self.slabs, use_current_stream=False))
+            else:
+                with torch.cuda.stream(stream):
+                    self.runs.append(SlabRun(p, r, world, transport=None, slabs=self.slabs))
         self.torch = torch
 
-    def exchange(self) -> None:
+    def _copies(self) -> None:
         runs = self.runs
-        for r in runs:
-            r.pack()
-        for r in runs:
-            r.problem.synchronize()
         for i, r in enumerate(runs):
             if 0 in r.sides:
                 r.recv[0].copy_(runs[i - 1].send[1])
             if 1 in r.sides:
                 r.recv[1].copy_(runs[i + 1].send[0])
+
+    def exchange(self) -> None:
+        runs = self.runs
+        if self.stream is not None:   # one stream orders everything
+            with self.torch.cuda.stream(self.stream):
+                for r in runs:
+                    r.pack()
+                self._copies()
+                for r in runs:
+                    r.unpack()
+            return
+        for r in runs:
+            r.pack()
+        for r in runs:
+            r.problem.synchronize()
+        self._copies()
         self.torch.cuda.synchronize(runs[0].device)
         for r in runs:
             r.unpack()

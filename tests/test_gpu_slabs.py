@@ -65,13 +65,13 @@ def _compare(whole, loc, nifaces):
             assert np.array_equal(a, b), "interface %d array %d" % (i, which)
 
 
-def _run(infile, precision, nslabs, nsteps, rule=None, slabs_plan=None):
+def _run(infile, precision, nslabs, nsteps, rule=None, slabs_plan=None, stream=None):
     whole = Problem(infile, precision)
     parts = [Problem(infile, precision) for _ in range(nslabs)]
     if rule is not None:
         for q in [whole] + parts:
             q.set_plastic_rule(rule)
-    loc = slabs.LocalSlabs(parts, slabs_plan)
+    loc = slabs.LocalSlabs(parts, slabs_plan, stream=stream)
     whole.step(nsteps)
     loc.step(nsteps)
     whole.synchronize()
@@ -87,6 +87,22 @@ def test_planar_slabs_match_whole(tmp_path, precision, nslabs):
     if precision == FP32:
         assert whole.set_volume_kernel(3) == 3   # the register-window kernel ran in both
     _compare(whole, loc, 1)
+
+
+def test_slabs_on_the_callers_stream(tmp_path):
+    # every slab launches on one torch stream and the ghost copies queue
+    # behind the packs on it: no host synchronisation between stages
+    import torch
+
+    tmp = str(tmp_path)
+    infile = _planar(tmp).write(os.path.join(tmp, "planar.in"))
+    stream = torch.cuda.Stream()
+    whole, loc = _run(infile, FP32, 3, 12, stream=stream)
+    _compare(whole, loc, 1)
+    for r in loc.runs:
+        r.release()   # back to the problem's own stream and the whole domain
+        r.problem.step(2)   # whole-domain steps (graph capture on the own stream) run again
+        r.problem.synchronize()
 
 
 def test_plastic_slabs_match_whole(tmp_path):
