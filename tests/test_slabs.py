@@ -81,6 +81,31 @@ class StandIn:
     def field(self, comp, absolute=False):
         return self.F[self.cur][comp].reshape(-1).copy()
 
+    # a fault: direction 1 spans every x plane (row a at x = a), direction 0
+    # lies on plane `xplane` (rows along the other axis); two components
+    fault_dir = 1
+    xplane = 31
+
+    def interface(self, i):
+        nx, m, _ = self.nx
+        if self.fault_dir == 1:
+            return 1, (0, 0, 0), (nx, m)
+        return 0, (self.xplane, 0, 0), (m, 1)
+
+    def fault(self, i, which):
+        f = self.F[self.cur]
+        if self.fault_dir == 1:
+            return np.concatenate([f[0], f[1] * which]).reshape(-1)
+        return np.concatenate([f[0, self.xplane], f[1, self.xplane] * which]).reshape(-1)
+
+    def energy(self, rate=True):
+        f = self.F[self.cur][:, self.x0:self.x1]
+        return {"kinetic": float(np.sum(f[0] ** 2)), "strain": float(np.sum(f[1] ** 2)),
+                "rate": float(np.sum(f[2])), "rate_scale": 1.0, "friction_power": float(np.sum(f[0] * f[1]))}
+
+
+ENERGY_KEYS = ("kinetic", "strain", "total", "rate", "friction_power")
+
 
 def _free_port():
     with socket.socket() as s:
@@ -102,6 +127,14 @@ def _rank(rank, world, port, outdir, nsteps):
             f = run.gather_field(comp)
             if rank == 0:
                 np.save(os.path.join(outdir, "f%d.npy" % comp), f)
+        for d in (1, 0):
+            p.fault_dir = d
+            f = run.gather_fault(0, 3)
+            if rank == 0:
+                np.save(os.path.join(outdir, "fault%d.npy" % d), f)
+        e = run.energy()
+        if rank == 0:
+            np.save(os.path.join(outdir, "energy.npy"), np.array([e[k] for k in ENERGY_KEYS]))
         with open(os.path.join(outdir, "r%d.txt" % rank), "w") as fh:
             fh.write("%d %d %d %d\n" % (run.x0, run.x1, run.exchanges, p.step_index))
     finally:
@@ -137,6 +170,13 @@ def test_gloo_slabs_match_whole_domain(world):
     for comp in range(3):
         got = np.load(os.path.join(out, "f%d.npy" % comp))
         assert np.array_equal(got, whole.field(comp))
+    for d in (1, 0):
+        whole.fault_dir = d
+        assert np.array_equal(np.load(os.path.join(out, "fault%d.npy" % d)), whole.fault(0, 3))
+    e = whole.energy()
+    e["total"] = e["kinetic"] + e["strain"]
+    np.testing.assert_allclose(np.load(os.path.join(out, "energy.npy")), [e[k] for k in ENERGY_KEYS],
+                               rtol=1e-13)
     rows = [open(os.path.join(out, "r%d.txt" % r)).read().split() for r in range(world)]
     assert [int(r[0]) for r in rows][0] == 0 and int(rows[-1][1]) == whole.nx[0]
     for r in rows:
