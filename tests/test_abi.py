@@ -65,3 +65,14 @@ def test_null_handle_is_an_argument_error():
     assert L.fdf_do_rk_stage(None, 0.1, 0, 0.0) == -1
     assert L.fdf_set_plastic_rule(None, 1) == -1
     assert L.fdf_get_fault_async(None, 0, 0, None) == -1
+    # x-slab entry points
+    assert L.fdf_step_stage(None, 0) == -1
+    assert L.fdf_set_x_range(None, 0, 16) == -1
+    assert L.fdf_pack_ghosts(None, 0, None) == -1
+    assert L.fdf_unpack_ghosts(None, 1, None) == -1
+    assert L.fdf_set_stream(None, 1, None) == -1
+    g, n, e = ctypes.c_int(), ctypes.c_longlong(), ctypes.c_int()
+    assert L.fdf_ghost_info(None, ctypes.byref(g), ctypes.byref(n), ctypes.byref(e)) == -1
+    lo, cnt = (ctypes.c_int * 3)(), (ctypes.c_int * 3)()
+    assert L.fdf_get_block(None, 0, lo, cnt) == -1
+    assert L.fdf_get_interface(None, 0, ctypes.byref(g), lo, cnt) == -1
