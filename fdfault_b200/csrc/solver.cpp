@@ -254,6 +254,13 @@ Solver::Solver(const std::string& infile, int precision, int device) : precision
 Solver::~Solver() {
     if (stream_) cudaStreamSynchronize(stream_);
     if (own_stream_ && own_stream_ != stream_) cudaStreamSynchronize(own_stream_);
+    if (copy_stream_) {
+        cudaStreamSynchronize(copy_stream_);
+        cudaStreamDestroy(copy_stream_);
+    }
+    for (auto& r : ring_busy_) cudaEventDestroy(r.done);
+    for (auto e : ring_events_) cudaEventDestroy(e);
+    if (ring_) cudaFree(ring_);
     out_.reset();
     for (void* p : owned_) cudaFree(p);
     for (void* p : {F_[0], F_[1], DF_, FP_, M_, J_, (void*)M64_, (void*)J64_, (void*)X_, (void*)S_, (void*)ABS_,
@@ -1250,7 +1257,10 @@ void Solver::solve() {
     cuda_check(cudaStreamSynchronize(stream_), "solve");
 }
 
-void Solver::synchronize() { cuda_check(cudaStreamSynchronize(stream_), "synchronize"); }
+void Solver::synchronize() {
+    cuda_check(cudaStreamSynchronize(stream_), "synchronize");
+    if (copy_stream_) cuda_check(cudaStreamSynchronize(copy_stream_), "synchronize read-back");
+}
 
 void Solver::energy(bool with_rate, double out[8]) {
     if (P_.plastic()) throw std::runtime_error("energy diagnostics cover elastic problems only");
@@ -1595,12 +1605,64 @@ void Solver::get_fault(int iface, int which, double* out) {
     fetch_to(fault_array(ifaces_[iface], which), (size_t)n * sizeof(double), out);
 }
 
+cudaEvent_t Solver::ring_event() {
+    if (!ring_events_.empty()) {
+        cudaEvent_t e = ring_events_.back();
+        ring_events_.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    return e;
+}
+
 void Solver::get_fault_async(int iface, int which, double* out) {
     long long n = fault_count(iface, which);
     if (n <= 0) throw std::runtime_error("no such fault array");
-    cuda_check(cudaMemcpyAsync(out, fault_array(ifaces_[iface], which), (size_t)n * sizeof(double),
-                               cudaMemcpyDeviceToHost, stream_),
-               "d2h");
+    const size_t bytes = (size_t)n * sizeof(double);
+    const double* src = fault_array(ifaces_[iface], which);
+    if (capturing_) throw std::runtime_error("get_fault_async inside a capture");
+    // ring of snapshots: room for a few steps of every fault array
+    const size_t need = (bytes + 255) & ~(size_t)255;
+    if (!ring_ || need > ring_cap_ / 4) {
+        if (ring_) {   // grow: wait for the copies out of the old ring first
+            cuda_check(cudaStreamSynchronize(copy_stream_), "ring");
+            for (auto& r : ring_busy_) ring_events_.push_back(r.done);
+            ring_busy_.clear();
+            cudaFree(ring_);
+            ring_ = nullptr;
+        }
+        size_t cap = (size_t)64 << 20;
+        while (cap < 4 * need) cap *= 2;
+        cuda_check(cudaMalloc(&ring_, cap), "cudaMalloc read-back ring");
+        ring_cap_ = cap;
+        ring_head_ = 0;
+        if (!copy_stream_)
+            cuda_check(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    }
+    if (ring_head_ + need > ring_cap_) ring_head_ = 0;
+    const size_t b0 = ring_head_, b1 = ring_head_ + need;
+    // a slot still being copied out: the snapshot waits for that copy (on the device)
+    for (size_t q = 0; q < ring_busy_.size();) {
+        if (ring_busy_[q].begin < b1 && b0 < ring_busy_[q].end) {
+            cuda_check(cudaStreamWaitEvent(stream_, ring_busy_[q].done, 0), "ring wait");
+            ring_events_.push_back(ring_busy_[q].done);
+            ring_busy_[q] = ring_busy_.back();
+            ring_busy_.pop_back();
+        } else {
+            q++;
+        }
+    }
+    cuda_check(cudaMemcpyAsync(ring_ + b0, src, bytes, cudaMemcpyDeviceToDevice, stream_), "snapshot");
+    cudaEvent_t snap = ring_event();
+    cuda_check(cudaEventRecord(snap, stream_), "event");
+    cuda_check(cudaStreamWaitEvent(copy_stream_, snap, 0), "ring wait");
+    ring_events_.push_back(snap);   // reusable once recorded again: waits already captured it
+    cuda_check(cudaMemcpyAsync(out, ring_ + b0, bytes, cudaMemcpyDeviceToHost, copy_stream_), "d2h");
+    cudaEvent_t done = ring_event();
+    cuda_check(cudaEventRecord(done, copy_stream_), "event");
+    ring_busy_.push_back({b0, b1, done});
+    ring_head_ = b1;
 }
 
 void Solver::set_fault(int iface, int which, const double* in) {

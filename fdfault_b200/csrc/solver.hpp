@@ -172,6 +172,18 @@ class Solver {
     int device_ = 0;
     cudaStream_t stream_ = nullptr;
     cudaStream_t own_stream_ = nullptr;   // created by the handle; stream_ may be the caller's
+    // get_fault_async: the array is snapshotted on stream_ into a device ring
+    // and copied to the host on copy_stream_, overlapping the steps queued after
+    struct RingCopy {
+        size_t begin, end;
+        cudaEvent_t done;   // the host copy out of [begin, end) finished
+    };
+    cudaStream_t copy_stream_ = nullptr;
+    char* ring_ = nullptr;
+    size_t ring_cap_ = 0, ring_head_ = 0;
+    std::vector<RingCopy> ring_busy_;
+    std::vector<cudaEvent_t> ring_events_;   // free events (timing disabled)
+    cudaEvent_t ring_event();
     bool slab_ = false;                   // x range narrower than the domain
     int xr0_ = 0, xr1_ = 0;               // updated global x planes [xr0_, xr1_)
     int stage_next_ = 0;                  // next stage of step_stage

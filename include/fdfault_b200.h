@@ -158,11 +158,13 @@ int fdf_fault_count(fdf_handle* h, int iface, int which, long long* n);
 int fdf_get_fault(fdf_handle* h, int iface, int which, double* out);
 /* Queues the same copy as fdf_get_fault behind the work already queued on the
  * handle and returns without waiting: `out` holds the values once a later
- * fdf_synchronize (or any call that waits) returns, and must stay valid until
- * then; page-locked `out` lets the copy overlap host work.  For reading a
- * step's fault output every step without stalling the next step's launch, in
- * the way the reference's output units read the friction arrays after each
- * step (src/outputunit.cpp:771-889). */
+ * fdf_synchronize returns, and must stay valid until then.  The array is
+ * snapshotted on the device (into a ring of at least 64 MB allocated by the
+ * first call) and copied to `out` on a second stream, so with page-locked
+ * `out` the copy overlaps the steps queued after it.  For reading a step's
+ * fault output every step without stalling the next step, in the way the
+ * reference's output units read the friction arrays after each step
+ * (src/outputunit.cpp:771-889). */
 int fdf_get_fault_async(fdf_handle* h, int iface, int which, double* out);
 int fdf_set_fault(fdf_handle* h, int iface, int which, const double* in);
 

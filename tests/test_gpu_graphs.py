@@ -80,3 +80,29 @@ def test_async_fault_read_matches_sync(tmp_path):
         for w, o in outs.items():
             assert np.array_equal(o, p.fault(0, w)), w
 
+
+def test_async_fault_reads_every_step_through_the_ring(tmp_path):
+    # a 100,001-node fault: six 0.8 MB arrays a step wrap the 64 MB snapshot
+    # ring after about 13 steps, so slots are reused while earlier copies may
+    # still be in flight; every step's values must match a synchronous read
+    import torch
+
+    tmp = str(tmp_path)
+    prob = P.mode2_rupture(nx=100001, ny=16, h=0.1, nt=40, name="ring", datadir=tmp + "/", nuc_half=1.0)
+    infile = prob.write(os.path.join(tmp, "ring.in"))
+    whichs = (fs.V, fs.U, fs.S, fs.SN, fs.VX, fs.SX)
+    nsteps = 30
+    with fs.Problem(infile, precision=fs.FP32) as p:
+        bufs = [[torch.empty(p.fault_count(0, w), dtype=torch.float64, pin_memory=True) for w in whichs]
+                for _ in range(nsteps)]
+        for s in range(nsteps):
+            p.step(1)
+            for w, b in zip(whichs, bufs[s]):
+                p.fault_async(0, w, b.numpy())
+        p.synchronize()
+    with fs.Problem(infile, precision=fs.FP32) as q:
+        for s in range(nsteps):
+            q.step(1)
+            for w, b in zip(whichs, bufs[s]):
+                assert np.array_equal(b.numpy(), q.fault(0, w)), (s, w)
+
