@@ -9,9 +9,13 @@ RK3 -- in FP32 fields with FP64 friction.  One "step" is one full RK3 time step
 dataset is involved.
 
 Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-Under torchrun each rank runs its own replica of the problem on its own GPU
-(the single-grid path does not shard), so ``value`` is the sum over ranks of
-node-stage updates divided by the slowest rank's time (weak scaling).
+                        [--decomp replicas|slabs]
+Under torchrun each rank runs by default its own replica of the problem on its
+own GPU, so ``value`` is the sum over ranks of node-stage updates divided by the
+slowest rank's time (weak scaling).  With ``--decomp slabs`` the ranks split
+one problem into x slabs and swap ghost planes over NCCL after every stage
+(fdfault_b200.slabs): ``value`` is the whole grid's node-stages over the
+slowest rank's time (strong scaling).
 """
 
 from __future__ import annotations

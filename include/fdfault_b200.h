@@ -116,7 +116,10 @@ int fdf_get_block(fdf_handle* h, int block, int* lo, int* n);
 int fdf_get_interface(fdf_handle* h, int iface, int* direction, int* lo, int* n);
 /* Launch on the caller's CUDA stream (own = 0; e.g. the stream a collective
  * library waits on) or the handle's own stream again (own = 1).  Waits for
- * the work already queued first. */
+ * the work already queued first.  The caller's stream must outlive its use
+ * by the handle (set own = 1 before destroying it), and fdf_step, which
+ * captures CUDA graphs on the stream, needs one other than the legacy
+ * default stream. */
 int fdf_set_stream(fdf_handle* h, int own, void* stream);
 
 /* Index of the next step to run. */
