@@ -1067,6 +1067,7 @@ void Solver::set_x_range(int x0, int x1) {
     const int nx = P_.nx[0];
     if (x0 < 0 || x1 > nx || x0 >= x1) throw std::runtime_error("set_x_range: need 0 <= x0 < x1 <= nx");
     const bool whole = (x0 == 0 && x1 == nx);
+    if (stage_next_ != 0) throw std::runtime_error("set_x_range: a step begun by step_stage is unfinished");
     if (!whole) {
         if (P_.ndim != 3) throw std::runtime_error("x slabs cover 3D problems");
         if (P_.cdiss > 0.) throw std::runtime_error("x slabs: artificial dissipation is not supported");
@@ -1086,6 +1087,8 @@ void Solver::set_x_range(int x0, int x1) {
                     throw std::runtime_error("set_x_range: cut at x = " + std::to_string(c) +
                                              " is within 16 planes of an x block face");
         }
+        // the planes packed for a neighbour lie inside the slab
+        if (x1 - x0 < SLAB_MARGIN) throw std::runtime_error("set_x_range: a slab spans at least 16 planes");
     }
     synchronize();
     for (auto& B : blocks_) {

@@ -157,6 +157,35 @@ def test_plan_balanced_and_inside_blocks():
     assert slabs.neighbours(0, 3) == {1: 1} and slabs.neighbours(1, 3) == {0: 0, 1: 2}
 
 
+def test_plan_properties_on_random_block_layouts():
+    # any x block layout and rank count: either a plan whose slabs tile
+    # [0, nx), each at least 16 planes wide with every cut at least 16 planes
+    # inside a block, or ValueError when no such plan exists for that count
+    rng = np.random.default_rng(11)
+    for _ in range(300):
+        sizes = rng.integers(20, 300, size=rng.integers(1, 4))
+        blocks, lo = [], 0
+        for n in sizes:
+            blocks.append((lo, int(n)))
+            lo += int(n)
+        nx = lo
+        world = int(rng.integers(1, 12))
+        try:
+            plan = slabs.plan_slabs(blocks, world)
+        except ValueError:
+            # one block of n planes has a plan exactly when n >= 16 * world
+            assert len(blocks) > 1 or nx < 16 * world
+            continue
+        assert len(blocks) > 1 or nx >= 16 * world or world == 1
+        assert len(plan) == world and plan[0][0] == 0 and plan[-1][1] == nx
+        assert all(a[1] == b[0] for a, b in zip(plan, plan[1:]))
+        assert all(b - a >= 16 for a, b in plan) or world == 1
+        for a, _ in plan[1:]:
+            assert any(lo0 + 16 <= a <= lo0 + n - 16 for lo0, n in blocks)
+        if len(blocks) == 1 and world > 1:   # one block: within a plane of the equal share
+            assert max(b - a for a, b in plan) - min(b - a for a, b in plan) <= 1
+
+
 @pytest.mark.parametrize("world", [2, 3])
 def test_gloo_slabs_match_whole_domain(world):
     nsteps = 4
